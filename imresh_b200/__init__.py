@@ -1,0 +1,264 @@
+"""imresh_b200 -- B200 shrink-wrap / HIO phase retrieval.
+
+Python front end over the C ABI of ``lib/libimresh_b200.so``
+(declared in ``include/imresh_b200.h``).  Every compute call goes through
+that library; there is no CPU fallback: if the library is missing the calls
+raise.  Device buffers may be given as torch CUDA tensors or raw pointers.
+
+Entry points mirror the reference's API for this path:
+
+* :func:`cuda_shrink_wrap` -- ``imresh::algorithms::cuda::cudaShrinkWrap``
+  (src/imresh/algorithms/cuda/cudaShrinkWrap.hpp:114-130): host buffer,
+  modulus in, object out, synchronous, returns 0 on success.
+* :class:`Plan` -- reusable device-resident reconstruction of one size.
+* :func:`fft2d`, :func:`gaussian_blur`, :func:`vector_max`,
+  :func:`gaussian_weights` -- the kernel-level operations of the path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libimresh_b200.so")
+HEADER_PATH = os.path.join(os.path.dirname(_HERE), "include", "imresh_b200.h")
+FLT_MIN = float(np.finfo(np.float32).tiny)
+_LIB = None
+
+
+class ImrError(RuntimeError):
+    def __init__(self, status: int, where: str = ""):
+        self.status = status
+        msg = f"{where}: {status_string(status)} ({status})"
+        detail = last_error()
+        if detail:
+            msg += f" [{detail}]"
+        super().__init__(msg)
+
+
+class CParams(C.Structure):
+    _fields_ = [("nCycles", C.c_uint), ("targetError", C.c_float), ("hioBeta", C.c_float),
+                ("intensityCutOffAutoCorel", C.c_float), ("intensityCutOff", C.c_float),
+                ("sigma0", C.c_float), ("sigmaChange", C.c_float), ("nHioCycles", C.c_uint)]
+
+
+@dataclass
+class Params:
+    """cudaShrinkWrap's parameters; 0 selects the reference's CUDA default."""
+    n_cycles: int = 0
+    target_error: float = 0.0
+    hio_beta: float = 0.0
+    cut_off_auto_corel: float = 0.0
+    cut_off: float = 0.0
+    sigma0: float = 0.0
+    sigma_change: float = 0.0
+    n_hio_cycles: int = 0
+
+    def c(self) -> CParams:
+        return CParams(self.n_cycles, self.target_error, self.hio_beta, self.cut_off_auto_corel,
+                       self.cut_off, self.sigma0, self.sigma_change, self.n_hio_cycles)
+
+
+def lib() -> C.CDLL:
+    """Load the native library (raises if it has not been built)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python __graft_entry__.py` "
+                           "(or `make -C imresh_b200/csrc`)")
+    L = C.CDLL(LIB_PATH)
+    vp, u, f, i = C.c_void_p, C.c_uint, C.c_float, C.c_int
+    L.imr_status_string.restype = C.c_char_p
+    L.imr_status_string.argtypes = [i]
+    L.imr_last_error.restype = C.c_char_p
+    L.imr_max_side.restype = u
+    L.imr_side_supported.argtypes = [u]
+    L.imr_cuda_shrink_wrap.argtypes = [vp, u, u, vp, u, u, u, f, f, f, f, f, f, u]
+    L.imr_plan_create.argtypes = [C.POINTER(vp), u, u, C.POINTER(CParams)]
+    L.imr_plan_execute.argtypes = [vp, vp, vp, vp]
+    L.imr_plan_execute_host.argtypes = [vp, vp, vp, vp]
+    L.imr_plan_stats.argtypes = [vp, vp, C.POINTER(i), vp]
+    L.imr_plan_launches.argtypes = [vp, C.POINTER(C.c_long)]
+    L.imr_plan_copy_state.argtypes = [vp, i, vp, vp]
+    L.imr_plan_destroy.argtypes = [vp]
+    L.imr_plan_profile.argtypes = [vp, i, vp, C.POINTER(f), C.POINTER(f)]
+    L.imr_plan_pass_bytes.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.imr_fft2d.argtypes = [vp, u, u, i, vp]
+    L.imr_gaussian_blur.argtypes = [vp, vp, u, u, C.c_double, i, vp]
+    L.imr_gaussian_weights.argtypes = [C.c_double, vp, i]
+    L.imr_vector_max.argtypes = [vp, C.c_size_t, C.POINTER(f), vp]
+    _LIB = L
+    return L
+
+
+def header_functions() -> list:
+    """Names of the functions include/imresh_b200.h declares."""
+    text = open(HEADER_PATH).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(imr_[a-z0-9_]+)\s*\(", text)))
+
+
+def status_string(rc: int) -> str:
+    return lib().imr_status_string(rc).decode()
+
+
+def last_error() -> str:
+    try:
+        return lib().imr_last_error().decode()
+    except Exception:   # library not loadable
+        return ""
+
+
+def _check(rc: int, where: str):
+    if rc != 0:
+        raise ImrError(rc, where)
+
+
+def _ptr(x) -> int:
+    if x is None:
+        return 0
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        if not x.is_contiguous():
+            raise ValueError("device tensor must be contiguous")
+        return x.data_ptr()
+    if isinstance(x, np.ndarray):
+        if not x.flags.c_contiguous:
+            raise ValueError("host array must be C-contiguous")
+        return x.ctypes.data
+    raise TypeError(f"cannot take a pointer of {type(x)}")
+
+
+def _stream(s) -> int:
+    if s is None:
+        try:
+            import torch
+            if torch.cuda.is_available():
+                return torch.cuda.current_stream().cuda_stream
+        except Exception:
+            pass
+        return 0
+    if isinstance(s, int):
+        return s
+    return s.cuda_stream
+
+
+def side_supported(n: int) -> bool:
+    return bool(lib().imr_side_supported(n))
+
+
+# ------------------------------------------------------------------ drop-in
+def cuda_shrink_wrap(io: np.ndarray, width: int, height: int, stream=0, n_blocks: int = 256,
+                     n_threads: int = 256, n_cycles: int = 0, target_error: float = 0.0,
+                     hio_beta: float = 0.0, cut_off_auto_corel: float = 0.0, cut_off: float = 0.0,
+                     sigma0: float = 0.0, sigma_change: float = 0.0, n_hio_cycles: int = 0) -> int:
+    """cudaShrinkWrap: ``io`` (float32, width*height, host) holds the Fourier
+    modulus on entry and Re(g') on return.  Returns 0 on success, else an
+    imr_status code (the reference returns 0 and exits the process on error)."""
+    if io.dtype != np.float32 or not io.flags.c_contiguous or io.size != width * height:
+        raise ValueError("io must be a C-contiguous float32 array of width*height values")
+    return lib().imr_cuda_shrink_wrap(io.ctypes.data, width, height, _stream(stream) if stream else 0,
+                                      n_blocks, n_threads, n_cycles, target_error, hio_beta,
+                                      cut_off_auto_corel, cut_off, sigma0, sigma_change,
+                                      n_hio_cycles)
+
+
+class Plan:
+    """Device-resident reconstruction plan for one (width, height, params)."""
+
+    def __init__(self, width: int, height: int, params: Params | None = None):
+        self.width, self.height = width, height
+        self.params = params or Params()
+        h = C.c_void_p()
+        cp = self.params.c()
+        _check(lib().imr_plan_create(C.byref(h), width, height, C.byref(cp)), "imr_plan_create")
+        self._h = h
+
+    def execute(self, d_modulus, d_out, stream=None):
+        _check(lib().imr_plan_execute(self._h, _ptr(d_modulus), _ptr(d_out), _stream(stream)),
+               "imr_plan_execute")
+
+    def execute_host(self, modulus: np.ndarray, out: np.ndarray | None = None, stream=None):
+        m = np.ascontiguousarray(modulus, dtype=np.float32)
+        if out is None:
+            out = np.empty_like(m)
+        _check(lib().imr_plan_execute_host(self._h, _ptr(m), _ptr(out), _stream(stream)),
+               "imr_plan_execute_host")
+        return out
+
+    def stats(self, stream=None):
+        """(cycles_done, per-cycle errors)."""
+        n = C.c_int()
+        cyc = max(self.params.n_cycles or 20, 1)
+        errs = np.zeros(cyc, np.float32)
+        _check(lib().imr_plan_stats(self._h, _stream(stream), C.byref(n), errs.ctypes.data),
+               "imr_plan_stats")
+        return n.value, errs[:n.value]
+
+    def launches(self) -> int:
+        n = C.c_long()
+        _check(lib().imr_plan_launches(self._h, C.byref(n)), "imr_plan_launches")
+        return n.value
+
+    def profile(self, iters: int = 20, stream=None):
+        """Mean (row pass ms, column pass ms) over `iters` HIO iterations."""
+        a, b = C.c_float(), C.c_float()
+        _check(lib().imr_plan_profile(self._h, iters, _stream(stream), C.byref(a), C.byref(b)),
+               "imr_plan_profile")
+        return a.value, b.value
+
+    def pass_bytes(self):
+        a, b = C.c_double(), C.c_double()
+        _check(lib().imr_plan_pass_bytes(self._h, C.byref(a), C.byref(b)), "imr_plan_pass_bytes")
+        return a.value, b.value
+
+    def state(self, what: str, stream=None) -> np.ndarray:
+        W, H = self.width, self.height
+        code, arr = {"mask": (0, np.zeros((H, W), np.uint8)),
+                     "x": (1, np.zeros((H, W), np.complex64)),
+                     "gprev": (2, np.zeros((H, W), np.complex64)),
+                     "blurred": (3, np.zeros((H, W), np.float32))}[what]
+        _check(lib().imr_plan_copy_state(self._h, code, arr.ctypes.data, _stream(stream)),
+               "imr_plan_copy_state")
+        return arr
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().imr_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------------ kernels
+def fft2d(d_data, width: int, height: int, sign: int, stream=None):
+    """In-place unnormalised 2D C2C transform of a device complex64 buffer."""
+    _check(lib().imr_fft2d(_ptr(d_data), width, height, sign, _stream(stream)), "imr_fft2d")
+
+
+def gaussian_blur(d_data, d_tmp, width: int, height: int, sigma: float, axes: int = 3, stream=None):
+    _check(lib().imr_gaussian_blur(_ptr(d_data), _ptr(d_tmp), width, height, float(sigma), axes,
+                                   _stream(stream)), "imr_gaussian_blur")
+
+
+def gaussian_weights(sigma: float) -> np.ndarray:
+    k = lib().imr_gaussian_weights(float(sigma), None, 0)
+    w = np.zeros(k, np.float32)
+    lib().imr_gaussian_weights(float(sigma), w.ctypes.data, k)
+    return w
+
+
+def vector_max(d_data, n: int, stream=None) -> float:
+    r = C.c_float()
+    _check(lib().imr_vector_max(_ptr(d_data), n, C.byref(r), _stream(stream)), "imr_vector_max")
+    return r.value

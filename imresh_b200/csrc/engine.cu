@@ -1,0 +1,698 @@
+// Host side of the engine: FFT plans, reconstruction plans (device buffers +
+// captured CUDA graph of one shrink-wrap cycle) and the C ABI declared in
+// include/imresh_b200.h.
+#include <cuda_runtime.h>
+#include <float.h>
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <map>
+#include <mutex>
+#include <vector>
+
+#include "imresh_b200.h"
+#include "kernels.cuh"
+#include "engine_host.hpp"
+
+namespace imr {
+
+thread_local char g_last_error[256] = "";
+
+void set_error(const char *what, cudaError_t e)
+{
+    snprintf(g_last_error, sizeof(g_last_error), "%s: %s", what, cudaGetErrorString(e));
+}
+
+// ---------------------------------------------------------------- lengths
+// Radix schedule: 8s first (4,4 or 4 or 2 for the remaining power of two),
+// then 3s, 5s and 7s.  Supported lengths: every 2^a 3^b 5^c 7^d up to
+// kMaxRuntimeSide (runtime-length kernels hold 8 values x 256 threads), and
+// the compile-time lengths 3072 and 4096 above it.
+bool factor_len(int n, std::vector<int> &rad)
+{
+    rad.clear();
+    if (n < 1 || n > (int)kMaxSide) return false;
+    if (n > kMaxRuntimeSide && n != 3072 && n != 4096) return false;
+    int m = n, k = 0;
+    while (m % 2 == 0) { m /= 2; ++k; }
+    while (k >= 3 && !(k == 4)) { rad.push_back(8); k -= 3; }
+    if (k == 4) { rad.push_back(4); rad.push_back(4); }
+    else if (k == 2) rad.push_back(4);
+    else if (k == 1) rad.push_back(2);
+    for (int p : {3, 5, 7})
+        while (m % p == 0) { rad.push_back(p); m /= p; }
+    return m == 1 && (int)rad.size() <= 14;
+}
+
+// Twiddle tables exp(-2 pi i t/n), t < n, computed in double; one per
+// (device, n), kept for the life of the process.
+static std::mutex g_tw_mu;
+static std::map<std::pair<int, int>, float2 *> g_tw;
+
+int make_fft_plan(int n, FftPlanDev &p)
+{
+    std::vector<int> rad;
+    if (!factor_len(n, rad)) return IMR_ERR_UNSUPPORTED_SIZE;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(g_tw_mu);
+    auto key = std::make_pair(dev, n);
+    auto it = g_tw.find(key);
+    float2 *d = nullptr;
+    if (it == g_tw.end()) {
+        std::vector<float2> h(n);
+        for (int t = 0; t < n; ++t) {
+            double a = -2.0 * M_PI * (double)t / (double)n;
+            h[t] = make_float2((float)cos(a), (float)sin(a));
+        }
+        cudaError_t e = cudaMalloc(&d, sizeof(float2) * n);
+        if (e != cudaSuccess) { set_error("cudaMalloc twiddles", e); return IMR_ERR_OUT_OF_MEMORY; }
+        e = cudaMemcpy(d, h.data(), sizeof(float2) * n, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) { set_error("cudaMemcpy twiddles", e); return IMR_ERR_CUDA; }
+        g_tw[key] = d;
+    } else {
+        d = it->second;
+    }
+    memset(&p, 0, sizeof(p));
+    p.n = n;
+    p.nrad = (int)rad.size();
+    for (size_t i = 0; i < rad.size(); ++i) p.rad[i] = rad[i];
+    p.tw = d;
+    return IMR_SUCCESS;
+}
+
+// calcGaussianKernel<float> (src/imresh/libs/calcGaussianKernel.cpp:42-91):
+// half width ceil(2.884402748387961466*sigma - 0.5); weights a*exp(i*i*b)
+// rounded to float, normalised by their double sum.
+int gaussian_weights(double sigma, float *w, int cap)
+{
+    const int half = (int)ceil(2.884402748387961466 * sigma - 0.5);
+    const int K = 2 * half + 1;
+    if (w == nullptr || K > cap) return K;
+    const double a = 1.0 / (sqrt(2.0 * M_PI) * sigma);
+    const double b = -1.0 / (2.0 * sigma * sigma);
+    double sum = 0;
+    for (int i = -half; i <= half; ++i) {
+        float v = (float)(a * exp(i * i * b));
+        w[half + i] = v;
+        sum += v;
+    }
+    for (int i = 0; i < K; ++i) w[i] = (float)((double)w[i] / sum);
+    return K;
+}
+
+// ---------------------------------------------------------------- dispatch
+// Kernels specialised at compile time for the lengths below; any other
+// supported length runs the runtime-length FFT (N = 0 instantiation).
+template <int N>
+static RowKernels row_set()
+{
+    return RowKernels{k_row_hio<true, N>, k_row_hio<false, N>, k_row_finish<N>, k_fft_rows<-1, N>,
+                      k_fft_rows<+1, N>, row_nb(N), row_threads(N)};
+}
+template <int N>
+static ColKernels col_set()
+{
+    return ColKernels{k_col<N>, k_col_init<N>, k_fft_cols<-1, N>, k_fft_cols<+1, N>, col_nb(N),
+                      col_threads(N)};
+}
+
+#define IMR_SIZES(X) X(64) X(128) X(192) X(256) X(384) X(512) X(768) X(1024) X(1536) X(2048) X(3072) X(4096)
+
+RowKernels row_kernels(int N)
+{
+    switch (N) {
+#define ROWCASE(n) case n: return row_set<n>();
+        IMR_SIZES(ROWCASE)
+#undef ROWCASE
+    default: {
+        RowKernels k = row_set<0>();
+        k.nb = (kRowVpt * kRowThreads) / N;
+        if (k.nb < 1) k.nb = 1;
+        return k;
+    }
+    }
+}
+
+ColKernels col_kernels(int N)
+{
+    switch (N) {
+#define COLCASE(n) case n: return col_set<n>();
+        IMR_SIZES(COLCASE)
+#undef COLCASE
+    default: {
+        ColKernels k = col_set<0>();
+        k.nb = (kColVpt * kColThreads) / N;
+        if (k.nb > 8) k.nb = 8;
+        if (k.nb < 1) k.nb = 1;
+        return k;
+    }
+    }
+}
+
+static std::mutex g_attr_mu;
+static std::vector<int> g_attr_done;
+
+// Opt every kernel into the device's largest dynamic shared-memory size
+// (opt-in limit minus the kernel's static shared memory).
+static int g_optin_smem = 0;
+
+template <class F>
+static cudaError_t allow_smem(F f)
+{
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, (const void *)f);
+    if (e != cudaSuccess) return e;
+    const int dyn = g_optin_smem - (int)fa.sharedSizeBytes;
+    return cudaFuncSetAttribute((const void *)f, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+}
+
+int ensure_kernel_attributes()
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(g_attr_mu);
+    for (int d : g_attr_done)
+        if (d == dev) return IMR_SUCCESS;
+    cudaError_t e = cudaDeviceGetAttribute(&g_optin_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    std::vector<int> sizes = {0};
+#define PUSH(n) sizes.push_back(n);
+    IMR_SIZES(PUSH)
+#undef PUSH
+    for (int n : sizes) {
+        RowKernels r = n ? row_kernels(n) : row_set<0>();
+        ColKernels c = n ? col_kernels(n) : col_set<0>();
+        if (e == cudaSuccess) e = allow_smem(r.hio_first);
+        if (e == cudaSuccess) e = allow_smem(r.hio);
+        if (e == cudaSuccess) e = allow_smem(r.finish);
+        if (e == cudaSuccess) e = allow_smem(r.fft_fwd);
+        if (e == cudaSuccess) e = allow_smem(r.fft_inv);
+        if (e == cudaSuccess) e = allow_smem(c.col);
+        if (e == cudaSuccess) e = allow_smem(c.init);
+        if (e == cudaSuccess) e = allow_smem(c.fft_fwd);
+        if (e == cudaSuccess) e = allow_smem(c.fft_inv);
+    }
+    if (e == cudaSuccess) e = allow_smem(k_hblur);
+    if (e != cudaSuccess) {
+        set_error("cudaFuncSetAttribute", e);
+        return IMR_ERR_CUDA;
+    }
+    g_attr_done.push_back(dev);
+    return IMR_SUCCESS;
+}
+
+void resolve_params(const imr_params *in, imr_params &p)
+{
+    // Defaults of the reference's CUDA driver (cudaShrinkWrap.cu:193-200).
+    if (in) p = *in;
+    else memset(&p, 0, sizeof(p));
+    if (p.nCycles == 0) p.nCycles = 20;
+    if (!(p.targetError > 0)) p.targetError = 1e-5f;
+    if (!(p.hioBeta > 0)) p.hioBeta = 0.9f;
+    if (!(p.intensityCutOffAutoCorel > 0)) p.intensityCutOffAutoCorel = 0.02f;
+    if (!(p.intensityCutOff > 0)) p.intensityCutOff = 0.2f;
+    if (!(p.sigma0 > 0)) p.sigma0 = 3.0f;
+    if (!(p.sigmaChange > 0)) p.sigmaChange = 0.01f;
+    if (p.nHioCycles == 0) p.nHioCycles = 20;
+}
+
+// Sigma of every cycle (sigma <- max(1.5, (1 - change)*sigma) after each
+// mask, in float: cudaShrinkWrap.cu:294) and its Gaussian weights.  Entry
+// n_cycles serves the final error-only pass.
+int build_weight_table(const imr_params &p, std::vector<float> &w, std::vector<int> &taps)
+{
+    w.assign((size_t)(p.nCycles + 1) * kTapStride, 0.f);
+    taps.assign(p.nCycles + 1, 1);
+    float sigma = p.sigma0;
+    for (unsigned c = 0; c <= p.nCycles; ++c) {
+        int K = gaussian_weights((double)sigma, &w[(size_t)c * kTapStride], kMaxTaps);
+        if (K > kMaxTaps) return IMR_ERR_INVALID_VALUE;
+        taps[c] = K;
+        sigma = fmaxf(1.5f, (1.0f - p.sigmaChange) * sigma);
+    }
+    return IMR_SUCCESS;
+}
+
+}  // namespace imr
+
+using namespace imr;
+
+// ==================================================================== plans
+struct imr_plan {
+    int dev = 0;
+    int W = 0, H = 0;
+    imr_params p{};
+    JobDev hj{};
+    JobDev *dj = nullptr;
+    JobState *st = nullptr;
+    void *arena = nullptr;
+    size_t smem_row = 0, smem_fin = 0, smem_col = 0;
+    cudaGraphExec_t gexec = nullptr;
+    cudaGraph_t graph = nullptr;
+    float2 *dbg_gprime = nullptr;
+    RowKernels rk{};
+    ColKernels ck{};
+};
+
+static int plan_launch_cycle(imr_plan *P, cudaStream_t s)
+{
+    const JobDev &J = P->hj;
+    const RowKernels &rk = P->rk;
+    const ColKernels &ck = P->ck;
+    rk.finish<<<J.n_row_tiles, rk.threads, P->smem_fin, s>>>(P->dj, nullptr, P->dbg_gprime);
+    k_vblur<<<J.n_vb_tiles, kVbThreads, 0, s>>>(P->dj, nullptr);
+    rk.hio_first<<<J.n_row_tiles, rk.threads, P->smem_row, s>>>(P->dj, nullptr);
+    ck.col<<<J.n_col_tiles, ck.threads, P->smem_col, s>>>(P->dj, nullptr);
+    for (int i = 1; i < J.n_hio; ++i) {
+        rk.hio<<<J.n_row_tiles, rk.threads, P->smem_row, s>>>(P->dj, nullptr);
+        ck.col<<<J.n_col_tiles, ck.threads, P->smem_col, s>>>(P->dj, nullptr);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error("kernel launch", e);
+        return IMR_ERR_CUDA;
+    }
+    return IMR_SUCCESS;
+}
+
+#define CK(call)                                  \
+    do {                                          \
+        cudaError_t e_ = (call);                  \
+        if (e_ != cudaSuccess) {                  \
+            set_error(#call, e_);                 \
+            return IMR_ERR_CUDA;                  \
+        }                                         \
+    } while (0)
+
+extern "C" {
+
+const char *imr_status_string(int s)
+{
+    switch (s) {
+    case IMR_SUCCESS: return "success";
+    case IMR_ERR_INVALID_VALUE: return "invalid value";
+    case IMR_ERR_UNSUPPORTED_SIZE: return "unsupported image size";
+    case IMR_ERR_OUT_OF_MEMORY: return "out of memory";
+    case IMR_ERR_CUDA: return "CUDA error";
+    case IMR_ERR_NOT_INITIALIZED: return "not initialised";
+    case IMR_ERR_QUEUE: return "task queue error";
+    default: return "unknown status";
+    }
+}
+
+const char *imr_last_error(void) { return g_last_error; }
+
+unsigned imr_max_side(void) { return kMaxSide; }
+
+int imr_side_supported(unsigned n)
+{
+    std::vector<int> r;
+    return factor_len((int)n, r) ? 1 : 0;
+}
+
+int imr_gaussian_weights(double sigma, float *h_w, int cap)
+{
+    if (!(sigma > 0)) return -1;
+    return gaussian_weights(sigma, h_w, cap);
+}
+
+int imr_plan_destroy(imr_plan *P)
+{
+    if (!P) return IMR_SUCCESS;
+    if (P->gexec) cudaGraphExecDestroy(P->gexec);
+    if (P->graph) cudaGraphDestroy(P->graph);
+    if (P->arena) cudaFree(P->arena);
+    if (P->dbg_gprime) cudaFree(P->dbg_gprime);
+    delete P;
+    return IMR_SUCCESS;
+}
+
+int imr_plan_create(imr_plan **out, unsigned W, unsigned H, const imr_params *params)
+{
+    if (!out || W == 0 || H == 0) return IMR_ERR_INVALID_VALUE;
+    *out = nullptr;
+    int rc = ensure_kernel_attributes();
+    if (rc) return rc;
+    imr_plan *P = new imr_plan();
+    cudaGetDevice(&P->dev);
+    P->W = (int)W;
+    P->H = (int)H;
+    resolve_params(params, P->p);
+    JobDev &J = P->hj;
+    J.W = (int)W;
+    J.H = (int)H;
+    if ((rc = make_fft_plan((int)W, J.prow)) || (rc = make_fft_plan((int)H, J.pcol))) {
+        delete P;
+        return rc;
+    }
+    std::vector<float> wt;
+    std::vector<int> taps;
+    if ((rc = build_weight_table(P->p, wt, taps))) {
+        delete P;
+        return rc;
+    }
+    P->rk = row_kernels(J.W);
+    P->ck = col_kernels(J.H);
+    J.rpc = P->rk.nb < J.H ? P->rk.nb : J.H;
+    J.cpc = P->ck.nb < J.W ? P->ck.nb : J.W;
+    J.n_row_tiles = (J.H + J.rpc - 1) / J.rpc;
+    J.n_col_tiles = (J.W + J.cpc - 1) / J.cpc;
+    J.vb_tiles_x = (J.W + kVbTileX - 1) / kVbTileX;
+    J.n_vb_tiles = J.vb_tiles_x * ((J.H + kVbTileY - 1) / kVbTileY);
+    J.beta = P->p.hioBeta;
+    J.cut_auto = P->p.intensityCutOffAutoCorel;
+    J.cut = P->p.intensityCutOff;
+    J.target = P->p.targetError;
+    J.n_cycles = (int)P->p.nCycles;
+    J.n_hio = (int)P->p.nHioCycles;
+    // shared memory sized for the compile-time tile (NB sequences), even when
+    // the image has fewer rows / columns than NB
+    P->smem_row = (size_t)P->rk.nb * J.W * sizeof(float2);
+    P->smem_fin = P->smem_row + (size_t)P->rk.nb * J.W * sizeof(float);
+    P->smem_col = (size_t)P->ck.nb * J.H * sizeof(float2);
+
+    // one arena: X, G (c64), M, hb, vb, out (f32), mask (u8), tables, state
+    const size_t N = (size_t)W * H;
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    size_t off = 0;
+    const size_t oX = off; off += al(N * 8);
+    const size_t oG = off; off += al(N * 8);
+    const size_t oM = off; off += al(N * 4);
+    const size_t oHB = off; off += al(N * 4);
+    const size_t oVB = off; off += al(N * 4);
+    const size_t oOut = off; off += al(N * 4);
+    const size_t oMask = off; off += al(N);
+    const size_t oW = off; off += al(wt.size() * 4);
+    const size_t oT = off; off += al(taps.size() * 4);
+    const size_t oEP = off; off += al((size_t)2 * J.n_row_tiles * 8);
+    const size_t oErr = off; off += al((size_t)(J.n_cycles + 1) * 4);
+    const size_t oSt = off; off += al(sizeof(JobState));
+    const size_t oJ = off; off += al(sizeof(JobDev));
+    cudaError_t e = cudaMalloc(&P->arena, off);
+    if (e != cudaSuccess) {
+        set_error("cudaMalloc plan arena", e);
+        delete P;
+        return IMR_ERR_OUT_OF_MEMORY;
+    }
+    char *a = (char *)P->arena;
+    J.X = (float2 *)(a + oX);
+    J.G = (float2 *)(a + oG);
+    J.M = (const float *)(a + oM);
+    J.hb = (float *)(a + oHB);
+    J.vb = (float *)(a + oVB);
+    J.out = (float *)(a + oOut);
+    J.mask = (uint8_t *)(a + oMask);
+    J.weights = (const float *)(a + oW);
+    J.ntaps = (const int *)(a + oT);
+    J.err_part = (double *)(a + oEP);
+    J.errors = (float *)(a + oErr);
+    J.st = (JobState *)(a + oSt);
+    P->st = J.st;
+    P->dj = (JobDev *)(a + oJ);
+    e = cudaMemcpy(a + oW, wt.data(), wt.size() * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(a + oT, taps.data(), taps.size() * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(P->dj, &J, sizeof(JobDev), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(a + oMask, 0, N);
+    if (e == cudaSuccess) e = cudaMemset(a + oErr, 0, (size_t)(J.n_cycles + 1) * 4);
+    if (e != cudaSuccess) {
+        set_error("plan upload", e);
+        imr_plan_destroy(P);
+        return IMR_ERR_CUDA;
+    }
+    // capture one shrink-wrap cycle as a graph
+    cudaStream_t cs;
+    e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        rc = plan_launch_cycle(P, cs);
+        cudaError_t e2 = cudaStreamEndCapture(cs, &P->graph);
+        if (rc == IMR_SUCCESS && e2 == cudaSuccess)
+            e = cudaGraphInstantiate(&P->gexec, P->graph, 0);
+        else if (e2 != cudaSuccess)
+            e = e2;
+    }
+    cudaStreamDestroy(cs);
+    if (e != cudaSuccess || rc != IMR_SUCCESS) {
+        if (e != cudaSuccess) set_error("graph capture", e);
+        imr_plan_destroy(P);
+        return rc ? rc : IMR_ERR_CUDA;
+    }
+    *out = P;
+    return IMR_SUCCESS;
+}
+
+int imr_plan_launches(imr_plan *P, long *launches)
+{
+    if (!P || !launches) return IMR_ERR_INVALID_VALUE;
+    *launches = 1 + (long)P->hj.n_cycles * (2 + 2L * P->hj.n_hio) + 2;
+    return IMR_SUCCESS;
+}
+
+int imr_plan_execute(imr_plan *P, const float *d_modulus, float *d_out, void *stream)
+{
+    if (!P || !d_modulus || !d_out) return IMR_ERR_INVALID_VALUE;
+    cudaStream_t s = (cudaStream_t)stream;
+    const JobDev &J = P->hj;
+    const size_t N = (size_t)P->W * P->H;
+    CK(cudaMemcpyAsync((void *)J.M, d_modulus, N * 4, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemsetAsync(P->st, 0, sizeof(JobState), s));
+    P->ck.init<<<J.n_col_tiles, P->ck.threads, P->smem_col, s>>>(P->dj, nullptr);
+    CK(cudaGetLastError());
+    for (int c = 0; c < J.n_cycles; ++c) CK(cudaGraphLaunch(P->gexec, s));
+    P->rk.finish<<<J.n_row_tiles, P->rk.threads, P->smem_fin, s>>>(P->dj, nullptr, P->dbg_gprime);
+    k_vblur<<<J.n_vb_tiles, kVbThreads, 0, s>>>(P->dj, nullptr);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(d_out, J.out, N * 4, cudaMemcpyDeviceToDevice, s));
+    return IMR_SUCCESS;
+}
+
+int imr_plan_execute_host(imr_plan *P, const float *h_modulus, float *h_out, void *stream)
+{
+    if (!P || !h_modulus || !h_out) return IMR_ERR_INVALID_VALUE;
+    cudaStream_t s = (cudaStream_t)stream;
+    const JobDev &J = P->hj;
+    const size_t N = (size_t)P->W * P->H;
+    CK(cudaMemcpyAsync((void *)J.M, h_modulus, N * 4, cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(P->st, 0, sizeof(JobState), s));
+    P->ck.init<<<J.n_col_tiles, P->ck.threads, P->smem_col, s>>>(P->dj, nullptr);
+    CK(cudaGetLastError());
+    for (int c = 0; c < J.n_cycles; ++c) CK(cudaGraphLaunch(P->gexec, s));
+    P->rk.finish<<<J.n_row_tiles, P->rk.threads, P->smem_fin, s>>>(P->dj, nullptr, P->dbg_gprime);
+    k_vblur<<<J.n_vb_tiles, kVbThreads, 0, s>>>(P->dj, nullptr);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(h_out, J.out, N * 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return IMR_SUCCESS;
+}
+
+int imr_plan_stats(imr_plan *P, void *stream, int *cycles_done, float *errors)
+{
+    if (!P) return IMR_ERR_INVALID_VALUE;
+    cudaStream_t s = (cudaStream_t)stream;
+    CK(cudaStreamSynchronize(s));
+    JobState st;
+    CK(cudaMemcpy(&st, P->st, sizeof(JobState), cudaMemcpyDeviceToHost));
+    if (cycles_done) *cycles_done = st.cycles_done;
+    if (errors) CK(cudaMemcpy(errors, P->hj.errors, sizeof(float) * P->hj.n_cycles, cudaMemcpyDeviceToHost));
+    return IMR_SUCCESS;
+}
+
+int imr_plan_copy_state(imr_plan *P, int what, void *h_dst, void *stream)
+{
+    if (!P || !h_dst) return IMR_ERR_INVALID_VALUE;
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t N = (size_t)P->W * P->H;
+    const void *src = nullptr;
+    size_t bytes = 0;
+    switch (what) {
+    case 0: src = P->hj.mask; bytes = N; break;
+    case 1: src = P->hj.X; bytes = N * 8; break;
+    case 2: src = P->hj.G; bytes = N * 8; break;
+    case 3: src = P->hj.vb; bytes = N * 4; break;
+    default: return IMR_ERR_INVALID_VALUE;
+    }
+    CK(cudaMemcpyAsync(h_dst, src, bytes, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return IMR_SUCCESS;
+}
+
+int imr_plan_profile(imr_plan *P, int iters, void *stream, float *ms_row, float *ms_col)
+{
+    if (!P || iters < 1 || !ms_row || !ms_col) return IMR_ERR_INVALID_VALUE;
+    cudaStream_t s = (cudaStream_t)stream;
+    const JobDev &J = P->hj;
+    std::vector<cudaEvent_t> ev(2 * iters + 1);
+    for (auto &e : ev) CK(cudaEventCreate(&e));
+    CK(cudaMemsetAsync(P->st, 0, sizeof(JobState), s));
+    CK(cudaEventRecord(ev[0], s));
+    for (int i = 0; i < iters; ++i) {
+        P->rk.hio<<<J.n_row_tiles, P->rk.threads, P->smem_row, s>>>(P->dj, nullptr);
+        CK(cudaEventRecord(ev[2 * i + 1], s));
+        P->ck.col<<<J.n_col_tiles, P->ck.threads, P->smem_col, s>>>(P->dj, nullptr);
+        CK(cudaEventRecord(ev[2 * i + 2], s));
+    }
+    CK(cudaGetLastError());
+    CK(cudaEventSynchronize(ev[2 * iters]));
+    double tr = 0, tc = 0;
+    for (int i = 0; i < iters; ++i) {
+        float a = 0, b = 0;
+        CK(cudaEventElapsedTime(&a, ev[2 * i], ev[2 * i + 1]));
+        CK(cudaEventElapsedTime(&b, ev[2 * i + 1], ev[2 * i + 2]));
+        tr += a;
+        tc += b;
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    *ms_row = (float)(tr / iters);
+    *ms_col = (float)(tc / iters);
+    return IMR_SUCCESS;
+}
+
+int imr_plan_pass_bytes(imr_plan *P, double *row_bytes, double *col_bytes)
+{
+    if (!P || !row_bytes || !col_bytes) return IMR_ERR_INVALID_VALUE;
+    const double N = (double)P->W * P->H;
+    *row_bytes = 33.0 * N;
+    *col_bytes = 20.0 * N;
+    return IMR_SUCCESS;
+}
+
+// ------------------------------------------------------------ drop-in
+int imr_cuda_shrink_wrap(float *io, unsigned W, unsigned H, void *stream, unsigned nBlocks,
+                         unsigned nThreads, unsigned nCycles, float targetError, float hioBeta,
+                         float cutAuto, float cut, float sigma0, float sigmaChange,
+                         unsigned nHio)
+{
+    (void)nBlocks;
+    (void)nThreads;
+    if (!io || W == 0 || H == 0) return IMR_ERR_INVALID_VALUE;
+    imr_params p{nCycles, targetError, hioBeta, cutAuto, cut, sigma0, sigmaChange, nHio};
+    imr_plan *P = nullptr;
+    int rc = plan_cache_acquire(W, H, &p, &P);
+    if (rc) return rc;
+    rc = imr_plan_execute_host(P, io, io, stream);
+    plan_cache_release(P);
+    return rc;
+}
+
+// ------------------------------------------------------------ kernel-level
+int imr_fft2d(void *d_data, unsigned W, unsigned H, int sign, void *stream)
+{
+    if (!d_data || W == 0 || H == 0 || (sign != 1 && sign != -1)) return IMR_ERR_INVALID_VALUE;
+    int rc = ensure_kernel_attributes();
+    if (rc) return rc;
+    FftPlanDev pr, pc;
+    if ((rc = make_fft_plan((int)W, pr)) || (rc = make_fft_plan((int)H, pc))) return rc;
+    const RowKernels rk = row_kernels((int)W);
+    const ColKernels ck = col_kernels((int)H);
+    const int rpc = rk.nb, cpc = ck.nb;
+    cudaStream_t s = (cudaStream_t)stream;
+    float2 *d = (float2 *)d_data;
+    const int nrt = ((int)H + rpc - 1) / rpc, nct = ((int)W + cpc - 1) / cpc;
+    const size_t sr = (size_t)rpc * W * 8, sc = (size_t)cpc * H * 8;
+    if (sign < 0) {
+        rk.fft_fwd<<<nrt, rk.threads, sr, s>>>(d, pr, (int)H, rpc);
+        ck.fft_fwd<<<nct, ck.threads, sc, s>>>(d, pc, (int)W, cpc);
+    } else {
+        ck.fft_inv<<<nct, ck.threads, sc, s>>>(d, pc, (int)W, cpc);
+        rk.fft_inv<<<nrt, rk.threads, sr, s>>>(d, pr, (int)H, rpc);
+    }
+    CK(cudaGetLastError());
+    return IMR_SUCCESS;
+}
+
+int imr_gaussian_blur(float *d_data, float *d_tmp, unsigned W, unsigned H, double sigma, int axes,
+                      void *stream)
+{
+    if (!d_data || W == 0 || H == 0 || !(sigma > 0) || axes < 1 || axes > 3) return IMR_ERR_INVALID_VALUE;
+    if ((axes & 2) && !d_tmp) return IMR_ERR_INVALID_VALUE;
+    if (W > 65536 || H > 65536) return IMR_ERR_UNSUPPORTED_SIZE;
+    int rc = ensure_kernel_attributes();
+    if (rc) return rc;
+    Taps t;
+    memset(&t, 0, sizeof(t));
+    const int K = gaussian_weights(sigma, t.w, kMaxTaps);
+    if (K > kMaxTaps) return IMR_ERR_INVALID_VALUE;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (axes & 1) k_hblur<<<H, kRowThreads, (size_t)W * 4, s>>>(d_data, (int)W, (int)H, t, K);
+    if (axes & 2) {
+        const int nt = (int)(((W + kVbTileX - 1) / kVbTileX) * ((H + kVbTileY - 1) / kVbTileY));
+        k_vblur_plain<<<nt, kVbThreads, 0, s>>>(d_data, d_tmp, (int)W, (int)H, t, K, nullptr);
+        CK(cudaMemcpyAsync(d_data, d_tmp, (size_t)W * H * 4, cudaMemcpyDeviceToDevice, s));
+    }
+    CK(cudaGetLastError());
+    return IMR_SUCCESS;
+}
+
+int imr_vector_max(const float *d, size_t n, float *h_max, void *stream)
+{
+    if (!d || !h_max) return IMR_ERR_INVALID_VALUE;
+    if (n == 0) {
+        *h_max = -FLT_MAX;
+        return IMR_SUCCESS;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned *dk = nullptr;
+    CK(cudaMallocAsync((void **)&dk, sizeof(unsigned), s));
+    CK(cudaMemsetAsync(dk, 0, sizeof(unsigned), s));
+    long blocks = (long)((n + 255) / 256);
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    k_vector_max<<<(unsigned)blocks, 256, 0, s>>>(d, (long)n, dk);
+    CK(cudaGetLastError());
+    unsigned key = 0;
+    CK(cudaMemcpyAsync(&key, dk, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    CK(cudaFreeAsync(dk, s));
+    CK(cudaStreamSynchronize(s));
+    unsigned u = (key & 0x80000000u) ? (key & 0x7fffffffu) : ~key;
+    memcpy(h_max, &u, 4);
+    return IMR_SUCCESS;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------ plan cache
+// Idle plans keyed by (device, W, H, parameters), so repeated drop-in calls
+// of one size reuse buffers and the captured graph.  Concurrent callers of
+// the same size get separate plans.
+namespace imr {
+struct PlanKey {
+    int dev;
+    unsigned W, H;
+    imr_params p;
+    bool operator<(const PlanKey &o) const { return memcmp(this, &o, sizeof(PlanKey)) < 0; }
+};
+static std::mutex g_cache_mu;
+static std::multimap<PlanKey, imr_plan *> g_idle;
+
+int plan_cache_acquire(unsigned W, unsigned H, const imr_params *params, imr_plan **out)
+{
+    PlanKey k;
+    memset(&k, 0, sizeof(k));
+    cudaGetDevice(&k.dev);
+    k.W = W;
+    k.H = H;
+    resolve_params(params, k.p);
+    {
+        std::lock_guard<std::mutex> lk(g_cache_mu);
+        auto it = g_idle.find(k);
+        if (it != g_idle.end()) {
+            *out = it->second;
+            g_idle.erase(it);
+            return IMR_SUCCESS;
+        }
+    }
+    return imr_plan_create(out, W, H, &k.p);
+}
+
+void plan_cache_release(imr_plan *P)
+{
+    PlanKey k;
+    memset(&k, 0, sizeof(k));
+    k.dev = P->dev;
+    k.W = (unsigned)P->W;
+    k.H = (unsigned)P->H;
+    k.p = P->p;
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    g_idle.insert(std::make_pair(k, P));
+}
+}  // namespace imr

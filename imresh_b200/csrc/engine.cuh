@@ -1,0 +1,76 @@
+// Device-side data model of the shrink-wrap / HIO engine.
+//
+// One reconstruction ("job") is the state the reference's cudaShrinkWrap keeps
+// in dpCurData / dpgPrevious / dpIntensity / dpIsMasked
+// (src/imresh/algorithms/cuda/cudaShrinkWrap.cu:203-214), re-laid out for
+// fused passes:
+//   X    complex64 [H][W]  the iterate between the row and column passes
+//                          (row-transformed g after a row pass; column-
+//                          projected, column-inverse-transformed after a
+//                          column pass)
+//   G    complex64 [H][W]  g_prev of the HIO update
+//   M    float32   [H][W]  the Fourier modulus (the caller's input)
+//   mask uint8     [H][W]  1 = outside the support (the reference's float 1.0)
+//   hb   float32   [H][W]  |g'| blurred along rows
+//   vb   float32   [H][W]  |g'| blurred along rows and columns
+//   out  float32   [H][W]  Re(g') -- the result
+// All per-cycle control (sigma weights, threshold, error, stop test) stays on
+// the device, so a reconstruction runs without host synchronisation.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "fft_dev.cuh"
+
+namespace imr {
+
+constexpr int kMaxTaps = 63;        // Gaussian kernel taps (half width <= 31)
+constexpr int kTapStride = 64;      // floats per cycle in the weight table
+constexpr int kRowThreads = 256;
+constexpr int kRowVpt = 8;          // complex values per thread per pass (rows, runtime length)
+constexpr int kColThreads = 256;
+constexpr int kColVpt = 8;          // complex values per thread per pass (columns, runtime length)
+constexpr int kVbTileX = 32;
+constexpr int kVbTileY = 64;
+constexpr int kVbThreads = 256;
+
+struct JobState {
+    int cycle;          // cycle whose mask is being built by finish/vblur
+    int hio_cycle;      // cycle whose HIO block is running
+    int stop;           // 1: finished; every later launch returns at once
+    int cycles_done;    // HIO blocks completed and error-tested
+    float thr;          // support threshold of the running cycle
+    unsigned max_bits;  // max of the blurred |g'| (float bits, values >= 0)
+    unsigned counter;   // last-block detection in the vertical blur pass
+    float last_error;
+};
+
+struct JobDev {
+    int W, H;
+    float2 *X;
+    float2 *G;
+    const float *M;
+    uint8_t *mask;
+    float *hb;
+    float *vb;
+    float *out;
+    FftPlanDev prow;    // length W
+    FftPlanDev pcol;    // length H
+    float beta, cut_auto, cut, target;
+    int n_cycles, n_hio;
+    const float *weights;   // [(n_cycles + 1) * kTapStride]
+    const int *ntaps;       // [n_cycles + 1]
+    double *err_part;       // [2 * n_row_tiles]  (sum mask*|g'|, sum mask)
+    float *errors;          // [n_cycles] error after each cycle
+    JobState *st;
+    int rpc;                // rows per row-pass CTA
+    int cpc;                // columns per column-pass CTA
+    int n_row_tiles, n_col_tiles, n_vb_tiles, vb_tiles_x;
+};
+
+// One CTA's assignment: job index and tile index within that job.
+struct WorkItem {
+    int job;
+    int tile;
+};
+
+}  // namespace imr

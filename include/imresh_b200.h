@@ -1,0 +1,138 @@
+/*
+ * imresh_b200 -- C ABI of the B200 shrink-wrap / hybrid-input-output (HIO)
+ * phase-retrieval engine (libimresh_b200.so).
+ *
+ * Plain C: pointers, sizes and status codes only.  Every entry point returns
+ * an imr_status; none of them exits or aborts the process (the reference
+ * prints and calls exit(EXIT_FAILURE) on any CUDA error,
+ * src/imresh/libs/cudacommon.cu:39-56).  `stream` arguments are cudaStream_t
+ * values passed as void* (NULL = the legacy default stream).
+ *
+ * Data convention (identical to the reference): an image is W*H float32,
+ * row-major with the width contiguous.  The input is the Fourier MODULUS |F|
+ * with the zero frequency at index 0 (the reference scales G' to it,
+ * src/imresh/algorithms/cuda/cudaVectorElementwise.cu:168-195); pass sqrt(I)
+ * for a measured intensity I.  The output is Re(g') of the last inverse
+ * transform, carrying the factor W*H of the unnormalised FFTs.
+ */
+#ifndef IMRESH_B200_H
+#define IMRESH_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum imr_status {
+    IMR_SUCCESS = 0,
+    IMR_ERR_INVALID_VALUE = 1,     /* NULL buffer, zero size, bad parameter   */
+    IMR_ERR_UNSUPPORTED_SIZE = 2,  /* W or H outside the supported lengths   */
+    IMR_ERR_OUT_OF_MEMORY = 3,     /* device or host allocation failed        */
+    IMR_ERR_CUDA = 4,              /* a CUDA runtime call failed              */
+    IMR_ERR_NOT_INITIALIZED = 5,   /* task queue used before imr_queue_init   */
+    IMR_ERR_QUEUE = 6              /* task queue / serving loop failure       */
+} imr_status;
+
+/* Parameters of one reconstruction, same meaning as the reference's
+ * cudaShrinkWrap arguments (src/imresh/algorithms/cuda/cudaShrinkWrap.hpp:114-130).
+ * A value <= 0 (== 0 for the counts) selects the reference's CUDA default
+ * (cudaShrinkWrap.cu:193-200): nCycles 20, targetError 1e-5, hioBeta 0.9,
+ * cutOffAutoCorel 0.02, cutOff 0.2, sigma0 3.0, sigmaChange 0.01,
+ * nHioCycles 20.  Pass targetError = FLT_MIN to run every cycle. */
+typedef struct imr_params {
+    unsigned nCycles;
+    float targetError;
+    float hioBeta;
+    float intensityCutOffAutoCorel;
+    float intensityCutOff;
+    float sigma0;
+    float sigmaChange;
+    unsigned nHioCycles;
+} imr_params;
+
+/* Human-readable name of a status code (static string). */
+const char *imr_status_string(int status);
+/* Detail of the last failed CUDA call on the calling thread ("" if none). */
+const char *imr_last_error(void);
+
+/* Largest supported image side and whether a side length is supported:
+ * lengths whose prime factors are all in {2, 3, 5, 7}, from 1 to 2048, plus
+ * 3072 and 4096. */
+unsigned imr_max_side(void);
+int imr_side_supported(unsigned n);
+
+/* ------------------------------------------------------------------------
+ * Drop-in for imresh::algorithms::cuda::cudaShrinkWrap
+ * (src/imresh/algorithms/cuda/cudaShrinkWrap.hpp:114-130, .cu:164-420).
+ * ioData: HOST buffer of W*H floats, modulus in, Re(g') out.  Synchronous:
+ * returns after the result is in ioData, like the reference (cu:403-407).
+ * nBlocks / nThreads are accepted for signature compatibility and ignored:
+ * the engine chooses its own launch shapes.  Returns 0 on success.
+ */
+int imr_cuda_shrink_wrap(float *ioData, unsigned W, unsigned H, void *stream,
+                         unsigned nBlocks, unsigned nThreads, unsigned nCycles,
+                         float targetError, float hioBeta,
+                         float intensityCutOffAutoCorel, float intensityCutOff,
+                         float sigma0, float sigmaChange, unsigned nHioCycles);
+
+/* ------------------------------------------------------------------------
+ * Reusable plan for one image size and parameter set (device buffers, FFT
+ * twiddles and the captured CUDA graph of one shrink-wrap cycle).  A plan
+ * serves one reconstruction at a time.
+ */
+typedef struct imr_plan imr_plan;
+
+int imr_plan_create(imr_plan **plan, unsigned W, unsigned H, const imr_params *params);
+/* Asynchronous on `stream`: reads W*H modulus floats from DEVICE memory
+ * d_modulus, writes W*H Re(g') floats to DEVICE memory d_out. */
+int imr_plan_execute(imr_plan *plan, const float *d_modulus, float *d_out, void *stream);
+/* Same through HOST buffers (pinned or pageable); synchronous. */
+int imr_plan_execute_host(imr_plan *plan, const float *h_modulus, float *h_out, void *stream);
+/* After execution (synchronises `stream`): cycles whose HIO block ran and
+ * was error-tested, and the error after each of them (errors may be NULL;
+ * otherwise room for nCycles floats). */
+int imr_plan_stats(imr_plan *plan, void *stream, int *cycles_done, float *errors);
+/* Kernel launches one execution issues (for launch accounting). */
+int imr_plan_launches(imr_plan *plan, long *launches);
+/* Debug state copies to HOST memory after execution (synchronise first):
+ * what = 0: mask (W*H bytes, 1 = outside the support)
+ *        1: X, the iterate between passes (W*H complex64)
+ *        2: g_prev (W*H complex64)
+ *        3: blurred |g'| of the last cycle (W*H float32) */
+int imr_plan_copy_state(imr_plan *plan, int what, void *h_dst, void *stream);
+/* Times the two passes of one HIO iteration on `stream` with CUDA events:
+ * runs `iters` (row pass, column pass) pairs on the plan's current state and
+ * returns the mean milliseconds of each pass.  Synchronous.  Leaves the
+ * plan's iterate changed; run it after imr_plan_execute, not inside one. */
+int imr_plan_profile(imr_plan *plan, int iters, void *stream, float *ms_row_pass,
+                     float *ms_col_pass);
+/* Algorithmic HBM bytes of one row pass and one column pass: every image
+ * array touched once (row: X, g_prev in; g_prev, X out; mask in = 33 B/px;
+ * column: X, modulus in; X out = 20 B/px). */
+int imr_plan_pass_bytes(imr_plan *plan, double *row_bytes, double *col_bytes);
+int imr_plan_destroy(imr_plan *plan);
+
+/* ------------------------------------------------------------------------
+ * Kernel-level entry points (device buffers, asynchronous on `stream`).
+ */
+/* Unnormalised 2D C2C transform in place; sign -1 forward, +1 inverse
+ * (cufftExecC2C FORWARD / INVERSE as used at cudaShrinkWrap.cu:232,319,343). */
+int imr_fft2d(void *d_data, unsigned W, unsigned H, int sign, void *stream);
+/* Separable Gaussian blur in place, clamp border, rows then columns
+ * (cudaGaussianBlur, src/imresh/algorithms/cuda/cudaGaussian.cu:1044-1057);
+ * axes: 1 rows only, 2 columns only, 3 both.  d_tmp: W*H floats of scratch. */
+int imr_gaussian_blur(float *d_data, float *d_tmp, unsigned W, unsigned H, double sigma,
+                      int axes, void *stream);
+/* Gaussian weights for sigma (calcGaussianKernel,
+ * src/imresh/libs/calcGaussianKernel.cpp:42-91); returns the tap count, and
+ * writes the weights when it is <= cap. */
+int imr_gaussian_weights(double sigma, float *h_weights, int cap);
+/* Global maximum of n floats (cudaVectorMax, cudaVectorReduce.cu:229-239);
+ * the result goes to HOST *h_max; synchronous. */
+int imr_vector_max(const float *d_data, size_t n, float *h_max, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

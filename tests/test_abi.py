@@ -1,0 +1,52 @@
+"""CPU-only checks of the drop-in boundary: the C-ABI library loads without a
+GPU, exports every function include/imresh_b200.h declares, and its host-side
+logic (status strings, supported lengths, Gaussian weights, parameter
+validation that needs no device) behaves as documented."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import imresh_b200 as imr
+import oracle
+
+
+def test_library_exports_every_declared_symbol():
+    L = imr.lib()
+    names = imr.header_functions()
+    assert len(names) >= 15
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_status_strings():
+    assert imr.status_string(0) == "success"
+    assert imr.status_string(2) == "unsupported image size"
+    assert imr.status_string(999) == "unknown status"
+
+
+@pytest.mark.parametrize("n,ok", [(1, True), (2, True), (64, True), (192, True), (210, True),
+                                  (343, True), (4096, True), (3072, True), (2187, False), (2400, False),
+                                  (2048, True), (4097, False), (11, False),
+                                  (1031, False), (0, False), (8192, False)])
+def test_side_supported(n, ok):
+    assert imr.side_supported(n) == ok
+    assert imr.lib().imr_max_side() == 4096
+
+
+@pytest.mark.parametrize("sigma", [0.1, 0.5, 1.0, 1.5, 2.2, 3.0, 4.0, 7.5])
+def test_gaussian_weights_match_oracle(sigma):
+    np.testing.assert_array_equal(imr.gaussian_weights(sigma), oracle.gaussian_weights(sigma))
+
+
+def test_invalid_arguments_rejected_without_device():
+    L = imr.lib()
+    buf = np.zeros(16, np.float32)
+    assert L.imr_cuda_shrink_wrap(None, 4, 4, None, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0) == 1
+    assert L.imr_cuda_shrink_wrap(buf.ctypes.data, 0, 4, None, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0) == 1
+    assert L.imr_fft2d(None, 4, 4, -1, None) == 1
+    assert L.imr_fft2d(buf.ctypes.data, 4, 4, 0, None) == 1
+    assert L.imr_gaussian_blur(None, None, 4, 4, 1.0, 3, None) == 1
+    h = C.c_void_p()
+    assert L.imr_plan_create(C.byref(h), 0, 4, None) == 1
+    assert L.imr_plan_destroy(None) == 0
