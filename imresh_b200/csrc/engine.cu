@@ -5,6 +5,7 @@
 #include <float.h>
 #include <math.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <map>
@@ -14,6 +15,7 @@
 #include "imresh_b200.h"
 #include "kernels.cuh"
 #include "engine_host.hpp"
+#include <cudaTypedefs.h>
 
 namespace imr {
 
@@ -108,14 +110,69 @@ int gaussian_weights(double sigma, float *w, int cap)
 template <int N>
 static RowKernels row_set()
 {
-    return RowKernels{k_row_hio<true, N>, k_row_hio<false, N>, k_row_finish<N>, k_fft_rows<-1, N>,
-                      k_fft_rows<+1, N>, row_nb(N), row_threads(N)};
+    if constexpr (N >= 16 && is_pow2(N))
+        return RowKernels{k_row_hio_r<true, N>, k_row_hio_r<false, N>, k_row_finish_r<N>,
+                          k_fft_rows_r<-1, N>, k_fft_rows_r<+1, N>, rrow_nb(N), rrow_threads(N),
+                          rrow_smem(N), k_row_hio_p<true, N>, k_row_hio_p<false, N>,
+                          prow_smem<true, N>(), prow_smem<false, N>()};
+    else if constexpr (N >= 8 && is_pow2(N))
+        return RowKernels{k_row_hio_r<true, N>, k_row_hio_r<false, N>, k_row_finish_r<N>,
+                          k_fft_rows_r<-1, N>, k_fft_rows_r<+1, N>, rrow_nb(N), rrow_threads(N),
+                          rrow_smem(N), nullptr, nullptr, 0, 0};
+    else
+        return RowKernels{k_row_hio<true, N>, k_row_hio<false, N>, k_row_finish<N>, k_fft_rows<-1, N>,
+                          k_fft_rows<+1, N>, row_nb(N), row_threads(N), 0, nullptr, nullptr, 0, 0};
 }
 template <int N>
 static ColKernels col_set()
 {
-    return ColKernels{k_col<N>, k_col_init<N>, k_fft_cols<-1, N>, k_fft_cols<+1, N>, col_nb(N),
-                      col_threads(N)};
+    if constexpr (N >= 16 && is_pow2(N))
+        return ColKernels{k_col_r<N>, k_col_init_r<N>, k_fft_cols_r<-1, N>, k_fft_cols_r<+1, N>,
+                          rcol_nb(N), rcol_threads(N), rcol_smem(N), k_col_p<N>, pcol_smem<N>(),
+                          pcol_box_rows(N), pcol_tma_m(N) ? 1 : 0};
+    else if constexpr (N >= 8 && is_pow2(N))
+        return ColKernels{k_col_r<N>, k_col_init_r<N>, k_fft_cols_r<-1, N>, k_fft_cols_r<+1, N>,
+                          rcol_nb(N), rcol_threads(N), rcol_smem(N), nullptr, 0, 0, 0};
+    else
+        return ColKernels{k_col<N>, k_col_init<N>, k_fft_cols<-1, N>, k_fft_cols<+1, N>, col_nb(N),
+                          col_threads(N), 0, nullptr, 0, 0, 0};
+}
+
+int persistent_grid(const void *kernel, int threads, int smem, int items)
+{
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess ||
+        per_sm < 1)
+        per_sm = 1;
+    long g = (long)per_sm * sms;
+    return (int)(g < items ? g : items);
+}
+
+static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+
+bool encode_tensor_map(CUtensorMap *map, const void *base, int W, int H, int elem, int box_w, int box_h)
+{
+    if (!g_encode) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn)
+            return false;
+        g_encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    }
+    if (((size_t)W * elem) % 16 != 0 || ((uintptr_t)base & 15) != 0 || (box_w * elem) % 16 != 0) return false;
+    if (box_w > 256 || box_h > 256 || box_w > W || box_h > H) return false;
+    cuuint64_t dims[2] = {(cuuint64_t)W, (cuuint64_t)H};
+    cuuint64_t strides[1] = {(cuuint64_t)W * elem};
+    cuuint32_t box[2] = {(cuuint32_t)box_w, (cuuint32_t)box_h};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = g_encode(map, elem == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+                          const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
 }
 
 #define IMR_SIZES(X) X(64) X(128) X(192) X(256) X(384) X(512) X(768) X(1024) X(1536) X(2048) X(3072) X(4096)
@@ -192,6 +249,9 @@ int ensure_kernel_attributes()
         if (e == cudaSuccess) e = allow_smem(c.init);
         if (e == cudaSuccess) e = allow_smem(c.fft_fwd);
         if (e == cudaSuccess) e = allow_smem(c.fft_inv);
+        if (e == cudaSuccess && r.p_hio) e = allow_smem(r.p_hio);
+        if (e == cudaSuccess && r.p_hio_first) e = allow_smem(r.p_hio_first);
+        if (e == cudaSuccess && c.p_col) e = allow_smem(c.p_col);
     }
     if (e == cudaSuccess) e = allow_smem(k_hblur);
     if (e != cudaSuccess) {
@@ -253,6 +313,8 @@ struct imr_plan {
     float2 *dbg_gprime = nullptr;
     RowKernels rk{};
     ColKernels ck{};
+    bool p_rows = false, p_cols = false;   // pipelined passes in use
+    int g_row_first = 0, g_row = 0, g_col = 0;
 };
 
 static int plan_launch_cycle(imr_plan *P, cudaStream_t s)
@@ -262,11 +324,19 @@ static int plan_launch_cycle(imr_plan *P, cudaStream_t s)
     const ColKernels &ck = P->ck;
     rk.finish<<<J.n_row_tiles, rk.threads, P->smem_fin, s>>>(P->dj, nullptr, P->dbg_gprime);
     k_vblur<<<J.n_vb_tiles, kVbThreads, 0, s>>>(P->dj, nullptr);
-    rk.hio_first<<<J.n_row_tiles, rk.threads, P->smem_row, s>>>(P->dj, nullptr);
-    ck.col<<<J.n_col_tiles, ck.threads, P->smem_col, s>>>(P->dj, nullptr);
-    for (int i = 1; i < J.n_hio; ++i) {
-        rk.hio<<<J.n_row_tiles, rk.threads, P->smem_row, s>>>(P->dj, nullptr);
-        ck.col<<<J.n_col_tiles, ck.threads, P->smem_col, s>>>(P->dj, nullptr);
+    for (int i = 0; i < J.n_hio; ++i) {
+        if (P->p_rows) {
+            if (i == 0)
+                rk.p_hio_first<<<P->g_row_first, rk.threads, rk.p_smem_first, s>>>(P->dj, nullptr, J.n_row_tiles);
+            else
+                rk.p_hio<<<P->g_row, rk.threads, rk.p_smem, s>>>(P->dj, nullptr, J.n_row_tiles);
+        } else {
+            (i == 0 ? rk.hio_first : rk.hio)<<<J.n_row_tiles, rk.threads, P->smem_row, s>>>(P->dj, nullptr);
+        }
+        if (P->p_cols)
+            ck.p_col<<<P->g_col, ck.threads, ck.p_smem, s>>>(P->dj, nullptr, J.n_col_tiles);
+        else
+            ck.col<<<J.n_col_tiles, ck.threads, P->smem_col, s>>>(P->dj, nullptr);
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
@@ -297,6 +367,7 @@ const char *imr_status_string(int s)
     case IMR_ERR_CUDA: return "CUDA error";
     case IMR_ERR_NOT_INITIALIZED: return "not initialised";
     case IMR_ERR_QUEUE: return "task queue error";
+    case IMR_ERR_DEVICE_TIMEOUT: return "device-side wait timed out";
     default: return "unknown status";
     }
 }
@@ -356,6 +427,9 @@ int imr_plan_create(imr_plan **out, unsigned W, unsigned H, const imr_params *pa
     P->ck = col_kernels(J.H);
     J.rpc = P->rk.nb < J.H ? P->rk.nb : J.H;
     J.cpc = P->ck.nb < J.W ? P->ck.nb : J.W;
+    P->p_rows = P->rk.p_hio != nullptr;
+    P->p_cols = P->ck.p_col != nullptr && J.W % 4 == 0 && J.W >= P->ck.nb;
+    if (P->p_cols) J.cpc = P->ck.nb;
     J.n_row_tiles = (J.H + J.rpc - 1) / J.rpc;
     J.n_col_tiles = (J.W + J.cpc - 1) / J.cpc;
     J.vb_tiles_x = (J.W + kVbTileX - 1) / kVbTileX;
@@ -368,9 +442,20 @@ int imr_plan_create(imr_plan **out, unsigned W, unsigned H, const imr_params *pa
     J.n_hio = (int)P->p.nHioCycles;
     // shared memory sized for the compile-time tile (NB sequences), even when
     // the image has fewer rows / columns than NB
-    P->smem_row = (size_t)P->rk.nb * J.W * sizeof(float2);
-    P->smem_fin = P->smem_row + (size_t)P->rk.nb * J.W * sizeof(float);
-    P->smem_col = (size_t)P->ck.nb * J.H * sizeof(float2);
+    if (P->rk.smem) {
+        P->smem_row = P->smem_fin = (size_t)P->rk.smem;   // norms reuse the FFT buffers
+    } else {
+        P->smem_row = (size_t)P->rk.nb * J.W * sizeof(float2);
+        P->smem_fin = P->smem_row + (size_t)P->rk.nb * J.W * sizeof(float);
+    }
+    P->smem_col = P->ck.smem ? (size_t)P->ck.smem : (size_t)P->ck.nb * J.H * sizeof(float2);
+    if (P->p_rows) {
+        P->g_row_first = persistent_grid((const void *)P->rk.p_hio_first, P->rk.threads, P->rk.p_smem_first,
+                                         J.n_row_tiles);
+        P->g_row = persistent_grid((const void *)P->rk.p_hio, P->rk.threads, P->rk.p_smem, J.n_row_tiles);
+    }
+    if (P->p_cols)
+        P->g_col = persistent_grid((const void *)P->ck.p_col, P->ck.threads, P->ck.p_smem, J.n_col_tiles);
 
     // one arena: X, G (c64), M, hb, vb, out (f32), mask (u8), tables, state
     const size_t N = (size_t)W * H;
@@ -410,6 +495,17 @@ int imr_plan_create(imr_plan **out, unsigned W, unsigned H, const imr_params *pa
     J.st = (JobState *)(a + oSt);
     P->st = J.st;
     P->dj = (JobDev *)(a + oJ);
+    if (P->p_cols) {
+        const int br = P->ck.p_box_rows;
+        bool okm = encode_tensor_map(&J.tmX, J.X, J.W, J.H, 8, P->ck.nb, br);
+        if (okm && P->ck.p_tma_m) okm = encode_tensor_map(&J.tmM, J.M, J.W, J.H, 4, P->ck.nb, br);
+        if (!okm) {   // shape the TMA unit cannot describe: per-tile column pass
+            P->p_cols = false;
+            J.cpc = P->ck.nb < J.W ? P->ck.nb : J.W;
+            J.n_col_tiles = (J.W + J.cpc - 1) / J.cpc;
+        }
+        J.use_tma_cols = P->p_cols ? 1 : 0;
+    }
     e = cudaMemcpy(a + oW, wt.data(), wt.size() * 4, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(a + oT, taps.data(), taps.size() * 4, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(P->dj, &J, sizeof(JobDev), cudaMemcpyHostToDevice);
@@ -494,6 +590,10 @@ int imr_plan_stats(imr_plan *P, void *stream, int *cycles_done, float *errors)
     JobState st;
     CK(cudaMemcpy(&st, P->st, sizeof(JobState), cudaMemcpyDeviceToHost));
     if (cycles_done) *cycles_done = st.cycles_done;
+    if (st.err) {
+        snprintf(g_last_error, sizeof(g_last_error), "a device-side copy wait timed out");
+        return IMR_ERR_DEVICE_TIMEOUT;
+    }
     if (errors) CK(cudaMemcpy(errors, P->hj.errors, sizeof(float) * P->hj.n_cycles, cudaMemcpyDeviceToHost));
     return IMR_SUCCESS;
 }
@@ -527,9 +627,15 @@ int imr_plan_profile(imr_plan *P, int iters, void *stream, float *ms_row, float 
     CK(cudaMemsetAsync(P->st, 0, sizeof(JobState), s));
     CK(cudaEventRecord(ev[0], s));
     for (int i = 0; i < iters; ++i) {
-        P->rk.hio<<<J.n_row_tiles, P->rk.threads, P->smem_row, s>>>(P->dj, nullptr);
+        if (P->p_rows)
+            P->rk.p_hio<<<P->g_row, P->rk.threads, P->rk.p_smem, s>>>(P->dj, nullptr, J.n_row_tiles);
+        else
+            P->rk.hio<<<J.n_row_tiles, P->rk.threads, P->smem_row, s>>>(P->dj, nullptr);
         CK(cudaEventRecord(ev[2 * i + 1], s));
-        P->ck.col<<<J.n_col_tiles, P->ck.threads, P->smem_col, s>>>(P->dj, nullptr);
+        if (P->p_cols)
+            P->ck.p_col<<<P->g_col, P->ck.threads, P->ck.p_smem, s>>>(P->dj, nullptr, J.n_col_tiles);
+        else
+            P->ck.col<<<J.n_col_tiles, P->ck.threads, P->smem_col, s>>>(P->dj, nullptr);
         CK(cudaEventRecord(ev[2 * i + 2], s));
     }
     CK(cudaGetLastError());
@@ -589,7 +695,8 @@ int imr_fft2d(void *d_data, unsigned W, unsigned H, int sign, void *stream)
     cudaStream_t s = (cudaStream_t)stream;
     float2 *d = (float2 *)d_data;
     const int nrt = ((int)H + rpc - 1) / rpc, nct = ((int)W + cpc - 1) / cpc;
-    const size_t sr = (size_t)rpc * W * 8, sc = (size_t)cpc * H * 8;
+    const size_t sr = rk.smem ? (size_t)rk.smem : (size_t)rpc * W * 8;
+    const size_t sc = ck.smem ? (size_t)ck.smem : (size_t)cpc * H * 8;
     if (sign < 0) {
         rk.fft_fwd<<<nrt, rk.threads, sr, s>>>(d, pr, (int)H, rpc);
         ck.fft_fwd<<<nct, ck.threads, sc, s>>>(d, pc, (int)W, cpc);

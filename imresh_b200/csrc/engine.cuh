@@ -19,6 +19,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <cuda.h>
 #include "fft_dev.cuh"
 
 namespace imr {
@@ -42,9 +43,13 @@ struct JobState {
     unsigned max_bits;  // max of the blurred |g'| (float bits, values >= 0)
     unsigned counter;   // last-block detection in the vertical blur pass
     float last_error;
+    int err;            // nonzero: a device-side wait gave up (see tma.cuh)
 };
 
-struct JobDev {
+struct alignas(64) JobDev {
+    CUtensorMap tmX;    // X as W x H 8-byte elements, box (cpc, rows)
+    CUtensorMap tmM;    // M as W x H floats, box (cpc, rows)
+    int use_tma_cols;   // 1: column pass reads tiles through tmX / tmM
     int W, H;
     float2 *X;
     float2 *G;

@@ -1,0 +1,199 @@
+// Register-resident FFT for power-of-two lengths (sm_100a).
+//
+// A sequence of length N is owned by Q = N/8 threads; thread l holds the
+// eight values at positions l + m*Q (m = 0..7) in v[m], before and after the
+// transform (natural order).  Each Stockham pass (radix R in {8,4,2}) runs
+// 8/R butterflies per thread entirely in registers; between passes the
+// values go through shared memory once (store, barrier, load), so a length
+// 2048 transform (radices 8,8,8,4) costs three shared-memory exchanges.
+// Because input and output sit at the same positions l + m*Q, an inverse
+// transform, a point-wise update and a forward transform chain in registers,
+// and global loads / stores are coalesced across the Q threads.
+//
+// Shared memory: two buffers (ping-pong, one barrier per exchange) of
+// padded length N + N/8 per sequence; the pad of one element per eight
+// spreads the strided stores of the early passes over all banks.
+#pragma once
+#include "fft_dev.cuh"
+
+namespace imr {
+
+__host__ __device__ constexpr bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+
+// padded index of element e
+__device__ __forceinline__ int pad8(int e) { return e + (e >> 3); }
+
+// Layout of NB sequences in one shared-memory buffer.
+//  rows:    sequence b at b*(N + N/8), element e at pad8(e)
+//  columns: element e of sequence b at pad8(e)*NB + b (one tile row contiguous)
+template <int N, int NB, bool COLS>
+struct SmemLayout {
+    static constexpr int kBuf = NB * (N + N / 8);   // float2 per buffer
+    __device__ __forceinline__ static int at(int b, int e)
+    {
+        if constexpr (COLS) return pad8(e) * NB + b;
+        else return b * (N + N / 8) + pad8(e);
+    }
+};
+
+// v[i] *= w^i for i = 1..R-1, w = table[t] (conjugated for S > 0); w^2 and
+// w^4 come from the table, the other powers from one product each.
+template <int R, int S>
+__device__ __forceinline__ void twiddle(float2 *u, const float2 *__restrict__ tw, int t, int n)
+{
+    if (t == 0) return;
+    auto ld = [&](int idx) {
+        float2 w = __ldg(tw + idx);
+        if (S > 0) w.y = -w.y;
+        return w;
+    };
+    const float2 w1 = ld(t);
+    if constexpr (R == 2) {
+        u[1] = cmul(u[1], w1);
+    } else if constexpr (R == 4) {
+        const float2 w2 = ld(2 * t);
+        u[1] = cmul(u[1], w1);
+        u[2] = cmul(u[2], w2);
+        u[3] = cmul(u[3], cmul(w1, w2));
+    } else {
+        const float2 w2 = ld(2 * t), w4 = ld(4 * t);
+        const float2 w3 = cmul(w1, w2);
+        u[1] = cmul(u[1], w1);
+        u[2] = cmul(u[2], w2);
+        u[3] = cmul(u[3], w3);
+        u[4] = cmul(u[4], w4);
+        u[5] = cmul(u[5], cmul(w1, w4));
+        u[6] = cmul(u[6], cmul(w2, w4));
+        u[7] = cmul(u[7], cmul(w3, w4));
+    }
+    (void)n;
+}
+
+template <int N, int NB, bool COLS, int S, int P, int NS>
+__device__ __forceinline__ void reg_passes(float2 (&v)[8], float2 *buf0, float2 *buf1, int b, int l,
+                                           const float2 *__restrict__ tw)
+{
+    constexpr RadixList L = radix_list(N);
+    if constexpr (P < L.n) {
+        constexpr int R = L.r[P];
+        constexpr int BPT = 8 / R;
+        constexpr int Q = N / 8;
+        constexpr int STEP = N / (NS * R);
+        static_assert(R == 2 || R == 4 || R == 8, "power-of-two radices only");
+        int kk[BPT];
+#pragma unroll
+        for (int i = 0; i < BPT; ++i) {
+            const int j = l + i * Q;
+            const int k = j & (NS - 1);
+            kk[i] = k;
+            float2 u[R];
+#pragma unroll
+            for (int q = 0; q < R; ++q) u[q] = v[i + q * BPT];
+            if constexpr (NS > 1) twiddle<R, S>(u, tw, k * STEP, N);
+            dftR<R, S>(u);
+#pragma unroll
+            for (int q = 0; q < R; ++q) v[i + q * BPT] = u[q];
+        }
+        if constexpr (P + 1 < L.n) {
+            using A = SmemLayout<N, NB, COLS>;
+            float2 *buf = (P & 1) ? buf1 : buf0;
+#pragma unroll
+            for (int i = 0; i < BPT; ++i) {
+                const int j = l + i * Q;
+                const int base = (j - kk[i]) * R + kk[i];
+#pragma unroll
+                for (int q = 0; q < R; ++q) buf[A::at(b, base + q * NS)] = v[i + q * BPT];
+            }
+            __syncthreads();
+#pragma unroll
+            for (int m = 0; m < 8; ++m) v[m] = buf[A::at(b, l + m * Q)];
+            reg_passes<N, NB, COLS, S, P + 1, NS * R>(v, buf0, buf1, b, l, tw);
+        }
+    }
+}
+
+// Unnormalised transform of the sequence held in v (see top of file).
+// Ends with a barrier, so the buffers may be reused right after.
+template <int N, int NB, bool COLS, int S>
+__device__ __forceinline__ void reg_fft(float2 (&v)[8], float2 *smem, int b, int l,
+                                        const float2 *__restrict__ tw)
+{
+    static_assert(is_pow2(N) && N >= 8, "register FFT needs a power-of-two length >= 8");
+    float2 *buf0 = smem;
+    float2 *buf1 = smem + SmemLayout<N, NB, COLS>::kBuf;
+    reg_passes<N, NB, COLS, S, 0, 1>(v, buf0, buf1, b, l, tw);
+    __syncthreads();
+}
+
+// ---- single-buffer variant with XOR-swizzled layouts -------------------------
+// Used by the pipelined kernels, whose exchange buffer is the TMA stage the
+// data arrived in.  Swizzles chosen by simulating the bank pattern of every
+// exchange (all power-of-two lengths): conflict-free, no padding.
+//  rows:    sequence b at b*N, element e at e ^ ((e >> 4) & 15)
+//  columns: element e of sequence b at (e ^ ((e >> 3) & (16/NB - 1)))*NB + b
+template <int N, int NB>
+struct RowSwz {
+    __device__ __forceinline__ static int at(int b, int e) { return b * N + (e ^ ((e >> 4) & 15)); }
+};
+template <int N, int NB>
+struct ColSwz {
+    static_assert(NB >= 1 && NB <= 16 && 16 % NB == 0, "column tile width must divide 16");
+    __device__ __forceinline__ static int at(int b, int e) { return (e ^ ((e >> 3) & (16 / NB - 1))) * NB + b; }
+};
+
+template <int N, class LAYOUT, int S, int P, int NS>
+__device__ __forceinline__ void reg_passes_1buf(float2 (&v)[8], float2 *buf, int b, int l,
+                                                const float2 *__restrict__ tw)
+{
+    constexpr RadixList L = radix_list(N);
+    if constexpr (P < L.n) {
+        constexpr int R = L.r[P];
+        constexpr int BPT = 8 / R;
+        constexpr int Q = N / 8;
+        constexpr int STEP = N / (NS * R);
+        int kk[BPT];
+#pragma unroll
+        for (int i = 0; i < BPT; ++i) {
+            const int j = l + i * Q;
+            const int k = j & (NS - 1);
+            kk[i] = k;
+            float2 u[R];
+#pragma unroll
+            for (int q = 0; q < R; ++q) u[q] = v[i + q * BPT];
+            if constexpr (NS > 1) twiddle<R, S>(u, tw, k * STEP, N);
+            dftR<R, S>(u);
+#pragma unroll
+            for (int q = 0; q < R; ++q) v[i + q * BPT] = u[q];
+        }
+        if constexpr (P + 1 < L.n) {
+            __syncthreads();   // earlier reads of buf are complete
+#pragma unroll
+            for (int i = 0; i < BPT; ++i) {
+                const int j = l + i * Q;
+                const int base = (j - kk[i]) * R + kk[i];
+#pragma unroll
+                for (int q = 0; q < R; ++q) buf[LAYOUT::at(b, base + q * NS)] = v[i + q * BPT];
+            }
+            __syncthreads();
+#pragma unroll
+            for (int m = 0; m < 8; ++m) v[m] = buf[LAYOUT::at(b, l + m * Q)];
+            reg_passes_1buf<N, LAYOUT, S, P + 1, NS * R>(v, buf, b, l, tw);
+        }
+    }
+}
+
+// Transform of the sequence in v through one exchange buffer.  Starts every
+// exchange with a barrier (so buf may still be read when it is called) and
+// leaves buf in use: callers synchronise before overwriting it.
+template <int N, class LAYOUT, int S>
+__device__ __forceinline__ void reg_fft_1buf(float2 (&v)[8], float2 *buf, int b, int l,
+                                             const float2 *__restrict__ tw)
+{
+    static_assert(is_pow2(N) && N >= 16, "pipelined FFT needs a power-of-two length >= 16");
+    reg_passes_1buf<N, LAYOUT, S, 0, 1>(v, buf, b, l, tw);
+}
+
+// shared memory (bytes) a register-FFT kernel needs
+__host__ __device__ constexpr int reg_smem_bytes(int N, int NB) { return 2 * NB * (N + N / 8) * 8; }
+
+}  // namespace imr

@@ -21,6 +21,8 @@
 // image and the threshold.
 #pragma once
 #include "engine.cuh"
+#include "fft_reg.cuh"
+#include "tma.cuh"
 
 namespace imr {
 
@@ -28,6 +30,13 @@ __device__ __forceinline__ WorkItem get_work(const WorkItem *wl)
 {
     if (wl) return wl[blockIdx.x];
     return WorkItem{0, (int)blockIdx.x};
+}
+
+// work item `item` of a persistent launch (a null list means job 0, tile item)
+__device__ __forceinline__ WorkItem get_work_at(const WorkItem *wl, int item)
+{
+    if (wl) return wl[item];
+    return WorkItem{0, item};
 }
 
 // ---- launch shapes ---------------------------------------------------------
@@ -480,6 +489,457 @@ __global__ void __launch_bounds__(256) k_vector_max(const float *d, long n, unsi
     if (threadIdx.x == 0) {
         for (int w = 1; w < 8; ++w) m = max(m, s[w]);
         atomicMax(key, m);
+    }
+}
+
+}  // namespace imr
+
+// ============================================================================
+// Power-of-two lengths: the same passes on the register-resident FFT
+// (fft_reg.cuh).  Thread (b, l) owns positions l + m*N/8 of sequence b.
+// ============================================================================
+namespace imr {
+
+__host__ __device__ constexpr int rrow_nb(int N) { return N <= 2048 ? 2048 / N : 1; }
+__host__ __device__ constexpr int rrow_threads(int N) { return rrow_nb(N) * N / 8; }
+__host__ __device__ constexpr int rcol_nb(int N) { return N <= 1024 ? (8192 / N < 16 ? 8192 / N : 16) : (N == 2048 ? 4 : 2); }
+__host__ __device__ constexpr int rcol_threads(int N) { return rcol_nb(N) * N / 8; }
+__host__ __device__ constexpr int rrow_smem(int N) { return reg_smem_bytes(N, rrow_nb(N)); }
+__host__ __device__ constexpr int rcol_smem(int N) { return reg_smem_bytes(N, rcol_nb(N)); }
+
+// X := inverse column FFT of (M, 0)
+template <int N>
+__global__ void __launch_bounds__(rcol_threads(N)) k_col_init_r(const JobDev *jobs, const WorkItem *wl)
+{
+    extern __shared__ float4 smem4[];
+    float2 *sm = reinterpret_cast<float2 *>(smem4);
+    constexpr int NB = rcol_nb(N), Q = N / 8;
+    const WorkItem wi = get_work(wl);
+    const JobDev &J = jobs[wi.job];
+    const int W = J.W;
+    const int b = threadIdx.x % NB, l = threadIdx.x / NB;
+    const int x = wi.tile * J.cpc + b;
+    const bool ok = b < J.cpc && x < W;
+    float2 v[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m)
+        v[m] = make_float2(ok ? J.M[(size_t)(l + m * Q) * W + x] : 0.f, 0.f);
+    reg_fft<N, NB, true, +1>(v, sm, b, l, J.pcol.tw);
+    if (ok) {
+#pragma unroll
+        for (int m = 0; m < 8; ++m) J.X[(size_t)(l + m * Q) * W + x] = v[m];
+    }
+}
+
+// column pass: forward column FFT, modulus projection, inverse column FFT
+template <int N>
+__global__ void __launch_bounds__(rcol_threads(N)) k_col_r(const JobDev *jobs, const WorkItem *wl)
+{
+    extern __shared__ float4 smem4[];
+    float2 *sm = reinterpret_cast<float2 *>(smem4);
+    constexpr int NB = rcol_nb(N), Q = N / 8;
+    const WorkItem wi = get_work(wl);
+    const JobDev &J = jobs[wi.job];
+    if (J.st->stop) return;
+    const int W = J.W;
+    const int b = threadIdx.x % NB, l = threadIdx.x / NB;
+    const int x = wi.tile * J.cpc + b;
+    const bool ok = b < J.cpc && x < W;
+    float2 v[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) v[m] = ok ? J.X[(size_t)(l + m * Q) * W + x] : make_float2(0.f, 0.f);
+    reg_fft<N, NB, true, -1>(v, sm, b, l, J.pcol.tw);
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        const float mod = ok ? J.M[(size_t)(l + m * Q) * W + x] : 0.f;
+        float nrm = cnorm_ref(v[m]);
+        if (nrm == 0.f) nrm = 1.f;
+        const float f = __fdiv_rn(mod, nrm);
+        v[m] = make_float2(__fmul_rn(v[m].x, f), __fmul_rn(v[m].y, f));
+    }
+    reg_fft<N, NB, true, +1>(v, sm, b, l, J.pcol.tw);
+    if (ok) {
+#pragma unroll
+        for (int m = 0; m < 8; ++m) J.X[(size_t)(l + m * Q) * W + x] = v[m];
+    }
+}
+
+// row pass: inverse row FFT, HIO update, forward row FFT (see k_row_hio)
+template <bool FIRST, int N>
+__global__ void __launch_bounds__(rrow_threads(N)) k_row_hio_r(const JobDev *jobs, const WorkItem *wl)
+{
+    extern __shared__ float4 smem4[];
+    float2 *sm = reinterpret_cast<float2 *>(smem4);
+    constexpr int Q = N / 8;
+    const WorkItem wi = get_work(wl);
+    const JobDev &J = jobs[wi.job];
+    JobState *st = J.st;
+    if (st->stop) return;
+    const int b = threadIdx.x / Q, l = threadIdx.x % Q;
+    const int y = wi.tile * J.rpc + b;
+    const bool ok = b < J.rpc && y < J.H;
+    const size_t base = (size_t)y * N;
+    float2 v[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) v[m] = ok ? J.X[base + l + m * Q] : make_float2(0.f, 0.f);
+    reg_fft<N, rrow_nb(N), false, +1>(v, sm, b, l, J.prow.tw);
+    const float beta = J.beta;
+    const float thr = st->thr;
+    const bool init_gprev = FIRST && st->hio_cycle == 0;
+    if (ok) {
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            const size_t idx = base + l + m * Q;
+            const float2 gp1 = v[m];
+            uint8_t msk;
+            if (FIRST) {
+                msk = J.vb[idx] < thr ? 1 : 0;
+                J.mask[idx] = msk;
+            } else {
+                msk = J.mask[idx];
+            }
+            const float2 gp = init_gprev ? gp1 : J.G[idx];
+            float2 g;
+            if (msk || gp1.x < 0.f)
+                g = make_float2(__fsub_rn(gp.x, __fmul_rn(beta, gp1.x)),
+                                __fsub_rn(gp.y, __fmul_rn(beta, gp1.y)));
+            else
+                g = gp1;
+            J.G[idx] = g;
+            v[m] = g;
+        }
+    }
+    reg_fft<N, rrow_nb(N), false, -1>(v, sm, b, l, J.prow.tw);
+    if (ok) {
+#pragma unroll
+        for (int m = 0; m < 8; ++m) J.X[base + l + m * Q] = v[m];
+    }
+}
+
+// once per cycle: inverse row FFT -> g'; out, error sums, |g'| blurred along rows
+template <int N>
+__global__ void __launch_bounds__(rrow_threads(N)) k_row_finish_r(const JobDev *jobs, const WorkItem *wl,
+                                                                 float2 *dbg_gprime)
+{
+    extern __shared__ float4 smem4[];
+    float2 *sm = reinterpret_cast<float2 *>(smem4);
+    constexpr int T = rrow_threads(N), Q = N / 8;
+    __shared__ float wsm[kTapStride];
+    __shared__ double red[2 * T / 32 > 2 ? 2 * T / 32 : 2];
+    const WorkItem wi = get_work(wl);
+    const JobDev &J = jobs[wi.job];
+    JobState *st = J.st;
+    if (st->stop) return;
+    const int c = st->cycle;
+    if (wi.tile == 0 && threadIdx.x == 0) st->max_bits = 0u;
+    const int b = threadIdx.x / Q, l = threadIdx.x % Q;
+    const int y = wi.tile * J.rpc + b;
+    const bool ok = b < J.rpc && y < J.H;
+    const size_t base = (size_t)y * N;
+    const int K = J.ntaps[c];
+    if (threadIdx.x < kTapStride) wsm[threadIdx.x] = J.weights[(size_t)c * kTapStride + threadIdx.x];
+    float2 v[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) v[m] = ok ? J.X[base + l + m * Q] : make_float2(0.f, 0.f);
+    reg_fft<N, rrow_nb(N), false, +1>(v, sm, b, l, J.prow.tw);
+    float *nrow = reinterpret_cast<float *>(sm) + b * N;   // buffers are free after reg_fft
+    double tot = 0.0, cnt = 0.0;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        const int e = l + m * Q;
+        const float nv = cnorm_ref(v[m]);
+        nrow[e] = nv;
+        if (ok) {
+            const size_t idx = base + e;
+            J.out[idx] = v[m].x;
+            if (dbg_gprime) dbg_gprime[idx] = v[m];
+            if (c > 0 && J.mask[idx]) {
+                tot += (double)nv;
+                cnt += 1.0;
+            }
+        }
+    }
+    block_sum2<T>(tot, cnt, red);   // includes barriers: nrow complete after it
+    if (threadIdx.x == 0) {
+        J.err_part[2 * wi.tile] = tot;
+        J.err_part[2 * wi.tile + 1] = cnt;
+    }
+    if (ok) {
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            const int e = l + m * Q;
+            J.hb[base + e] = hblur_at(nrow, N, e, wsm, K);
+        }
+    }
+}
+
+// plain 2D transform passes
+template <int S, int N>
+__global__ void __launch_bounds__(rrow_threads(N)) k_fft_rows_r(float2 *data, FftPlanDev p, int H, int rpc)
+{
+    extern __shared__ float4 smem4[];
+    float2 *sm = reinterpret_cast<float2 *>(smem4);
+    constexpr int Q = N / 8;
+    const int b = threadIdx.x / Q, l = threadIdx.x % Q;
+    const int y = blockIdx.x * rpc + b;
+    const bool ok = b < rpc && y < H;
+    const size_t base = (size_t)y * N;
+    float2 v[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) v[m] = ok ? data[base + l + m * Q] : make_float2(0.f, 0.f);
+    reg_fft<N, rrow_nb(N), false, S>(v, sm, b, l, p.tw);
+    if (ok) {
+#pragma unroll
+        for (int m = 0; m < 8; ++m) data[base + l + m * Q] = v[m];
+    }
+}
+
+template <int S, int N>
+__global__ void __launch_bounds__(rcol_threads(N)) k_fft_cols_r(float2 *data, FftPlanDev p, int W, int cpc)
+{
+    extern __shared__ float4 smem4[];
+    float2 *sm = reinterpret_cast<float2 *>(smem4);
+    constexpr int NB = rcol_nb(N), Q = N / 8;
+    const int b = threadIdx.x % NB, l = threadIdx.x / NB;
+    const int x = blockIdx.x * cpc + b;
+    const bool ok = b < cpc && x < W;
+    float2 v[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) v[m] = ok ? data[(size_t)(l + m * Q) * W + x] : make_float2(0.f, 0.f);
+    reg_fft<N, NB, true, S>(v, sm, b, l, p.tw);
+    if (ok) {
+#pragma unroll
+        for (int m = 0; m < 8; ++m) data[(size_t)(l + m * Q) * W + x] = v[m];
+    }
+}
+
+}  // namespace imr
+
+// ============================================================================
+// Pipelined (persistent) passes for power-of-two lengths.
+//
+// Each CTA loops over its work items (blockIdx.x, + gridDim.x, ...).  Two
+// shared-memory stages alternate: while the CTA transforms item i in one
+// stage, the TMA engine copies item i+1 into the other (1D bulk copies for
+// rows, 2D tensor-map tiles for columns), so HBM traffic stays in flight
+// across the compute.  The FFT exchanges reuse the stage the item arrived
+// in (swizzled, see fft_reg.cuh).
+// ============================================================================
+namespace imr {
+
+__host__ __device__ constexpr int round16(int b) { return (b + 15) & ~15; }
+__host__ __device__ constexpr int round128(int b) { return (b + 127) & ~127; }
+
+// ---- rows -------------------------------------------------------------------
+// stage: X rows (complex) | G rows (complex) | mask rows (u8) or blurred rows (f32)
+template <bool FIRST, int N>
+__host__ __device__ constexpr int prow_stage_bytes()
+{
+    return round128(2 * rrow_nb(N) * N * 8 + (FIRST ? rrow_nb(N) * N * 4 : round16(rrow_nb(N) * N)));
+}
+template <bool FIRST, int N>
+__host__ __device__ constexpr int prow_smem() { return 128 + 2 * prow_stage_bytes<FIRST, N>(); }
+
+__device__ __forceinline__ bool job_live(const JobDev *jobs, const WorkItem *wl, int item)
+{
+    const WorkItem wi = get_work_at(wl, item);
+    return jobs[wi.job].st->stop == 0;
+}
+
+template <bool FIRST, int N>
+__global__ void __launch_bounds__(rrow_threads(N)) k_row_hio_p(const JobDev *jobs, const WorkItem *wl,
+                                                              int n_items)
+{
+    extern __shared__ __align__(128) unsigned char sbuf[];
+    constexpr int NB = rrow_nb(N), Q = N / 8;
+    constexpr int XB = NB * N * 8;
+    constexpr int STAGE = prow_stage_bytes<FIRST, N>();
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sbuf);
+    unsigned char *stages = sbuf + 128;
+    const int b = threadIdx.x / Q, l = threadIdx.x % Q;
+
+    auto next_live = [&](int it) {
+        while (it < n_items && !job_live(jobs, wl, it)) it += gridDim.x;
+        return it;
+    };
+    auto issue = [&](int item, int s) {   // one thread
+        const WorkItem wi = get_work_at(wl, item);
+        const JobDev &J = jobs[wi.job];
+        const int y0 = wi.tile * J.rpc;
+        const int nr = min(J.rpc, J.H - y0);
+        const uint32_t xb = (uint32_t)(nr * N * 8);
+        const uint32_t mb = FIRST ? (uint32_t)(nr * N * 4) : (uint32_t)round16(nr * N);
+        unsigned char *st = stages + s * STAGE;
+        mbar_arrive_expect_tx(&bars[s], 2 * xb + mb);
+        tma_load_1d(st, J.X + (size_t)y0 * N, xb, &bars[s]);
+        tma_load_1d(st + XB, J.G + (size_t)y0 * N, xb, &bars[s]);
+        if (FIRST) tma_load_1d(st + 2 * XB, J.vb + (size_t)y0 * N, mb, &bars[s]);
+        else tma_load_1d(st + 2 * XB, J.mask + (size_t)y0 * N, mb, &bars[s]);
+    };
+
+    if (threadIdx.x == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    int item = next_live(blockIdx.x);
+    if (threadIdx.x == 0 && item < n_items) issue(item, 0);
+    for (int k = 0; item < n_items; ++k) {
+        const int nxt = next_live(item + gridDim.x);
+        const int s = k & 1;
+        if (threadIdx.x == 0 && nxt < n_items) {
+            fence_proxy_async_smem();
+            issue(nxt, s ^ 1);
+        }
+        const WorkItem wi = get_work_at(wl, item);
+        const JobDev &J = jobs[wi.job];
+        JobState *st = J.st;
+        const bool landed = mbar_wait(&bars[s], (uint32_t)((k >> 1) & 1));
+        if (__syncthreads_or(!landed)) {
+            if (threadIdx.x == 0) {
+                atomicExch(&st->err, 1);
+                if (nxt < n_items) mbar_wait(&bars[s ^ 1], (uint32_t)(((k + 1) >> 1) & 1));
+            }
+            return;
+        }
+        unsigned char *stg = stages + s * STAGE;
+        float2 *sX = reinterpret_cast<float2 *>(stg);
+        const float2 *sG = reinterpret_cast<const float2 *>(stg + XB);
+        const int y = wi.tile * J.rpc + b;
+        const bool ok = b < J.rpc && y < J.H;
+        const size_t base = (size_t)y * N;
+        float2 v[8];
+#pragma unroll
+        for (int m = 0; m < 8; ++m) v[m] = sX[b * N + l + m * Q];
+        reg_fft_1buf<N, RowSwz<N, NB>, +1>(v, sX, b, l, J.prow.tw);
+        const float beta = J.beta;
+        const float thr = st->thr;
+        const bool init_gprev = FIRST && st->hio_cycle == 0;
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            const int e = b * N + l + m * Q;
+            const float2 gp1 = v[m];
+            uint8_t msk;
+            if constexpr (FIRST) msk = reinterpret_cast<const float *>(stg + 2 * XB)[e] < thr ? 1 : 0;
+            else msk = (stg + 2 * XB)[e];
+            const float2 gp = init_gprev ? gp1 : sG[e];
+            float2 g;
+            if (msk || gp1.x < 0.f)
+                g = make_float2(__fsub_rn(gp.x, __fmul_rn(beta, gp1.x)),
+                                __fsub_rn(gp.y, __fmul_rn(beta, gp1.y)));
+            else
+                g = gp1;
+            if (ok) {
+                J.G[base + l + m * Q] = g;
+                if constexpr (FIRST) J.mask[base + l + m * Q] = msk;
+            }
+            v[m] = g;
+        }
+        reg_fft_1buf<N, RowSwz<N, NB>, -1>(v, sX, b, l, J.prow.tw);
+        if (ok) {
+#pragma unroll
+            for (int m = 0; m < 8; ++m) J.X[base + l + m * Q] = v[m];
+        }
+        fence_proxy_async_smem();
+        __syncthreads();   // stage s is free for the copy issued next iteration
+        item = nxt;
+    }
+}
+
+// ---- columns ------------------------------------------------------------------
+// stage: X tile [N][NB] complex | M tile [N][NB] float (when NB*4 >= 16)
+__host__ __device__ constexpr int pcol_box_rows(int N) { return N < 256 ? N : 256; }
+__host__ __device__ constexpr bool pcol_tma_m(int N) { return rcol_nb(N) * 4 >= 16; }
+template <int N>
+__host__ __device__ constexpr int pcol_stage_bytes()
+{
+    return round128(rcol_nb(N) * N * 8 + (pcol_tma_m(N) ? rcol_nb(N) * N * 4 : 0));
+}
+template <int N>
+__host__ __device__ constexpr int pcol_smem() { return 128 + 2 * pcol_stage_bytes<N>(); }
+
+template <int N>
+__global__ void __launch_bounds__(rcol_threads(N)) k_col_p(const JobDev *jobs, const WorkItem *wl, int n_items)
+{
+    extern __shared__ __align__(128) unsigned char sbuf[];
+    constexpr int NB = rcol_nb(N), Q = N / 8;
+    constexpr int XB = NB * N * 8;
+    constexpr int BR = pcol_box_rows(N);
+    constexpr bool TM = pcol_tma_m(N);
+    constexpr int STAGE = pcol_stage_bytes<N>();
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sbuf);
+    unsigned char *stages = sbuf + 128;
+    const int b = threadIdx.x % NB, l = threadIdx.x / NB;
+
+    auto next_live = [&](int it) {
+        while (it < n_items && !job_live(jobs, wl, it)) it += gridDim.x;
+        return it;
+    };
+    auto issue = [&](int item, int s) {
+        const WorkItem wi = get_work_at(wl, item);
+        const JobDev &J = jobs[wi.job];
+        const int x0 = wi.tile * NB;
+        unsigned char *st = stages + s * STAGE;
+        mbar_arrive_expect_tx(&bars[s], (uint32_t)(XB + (TM ? NB * N * 4 : 0)));
+        for (int r0 = 0; r0 < N; r0 += BR) {
+            tma_load_2d(st + (size_t)r0 * NB * 8, &J.tmX, x0, r0, &bars[s]);
+            if constexpr (TM) tma_load_2d(st + XB + (size_t)r0 * NB * 4, &J.tmM, x0, r0, &bars[s]);
+        }
+    };
+
+    if (threadIdx.x == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    int item = next_live(blockIdx.x);
+    if (threadIdx.x == 0 && item < n_items) issue(item, 0);
+    for (int k = 0; item < n_items; ++k) {
+        const int nxt = next_live(item + gridDim.x);
+        const int s = k & 1;
+        if (threadIdx.x == 0 && nxt < n_items) {
+            fence_proxy_async_smem();
+            issue(nxt, s ^ 1);
+        }
+        const WorkItem wi = get_work_at(wl, item);
+        const JobDev &J = jobs[wi.job];
+        const bool landed = mbar_wait(&bars[s], (uint32_t)((k >> 1) & 1));
+        if (__syncthreads_or(!landed)) {
+            if (threadIdx.x == 0) {
+                atomicExch(&J.st->err, 1);
+                if (nxt < n_items) mbar_wait(&bars[s ^ 1], (uint32_t)(((k + 1) >> 1) & 1));
+            }
+            return;
+        }
+        unsigned char *stg = stages + s * STAGE;
+        float2 *sX = reinterpret_cast<float2 *>(stg);
+        const int W = J.W;
+        const int x = wi.tile * NB + b;
+        const bool ok = x < W;
+        float2 v[8];
+#pragma unroll
+        for (int m = 0; m < 8; ++m) v[m] = sX[(l + m * Q) * NB + b];
+        reg_fft_1buf<N, ColSwz<N, NB>, -1>(v, sX, b, l, J.pcol.tw);
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            float mod;
+            if constexpr (TM) mod = reinterpret_cast<const float *>(stg + XB)[(l + m * Q) * NB + b];
+            else mod = ok ? J.M[(size_t)(l + m * Q) * W + x] : 0.f;
+            float nrm = cnorm_ref(v[m]);
+            if (nrm == 0.f) nrm = 1.f;
+            const float f = __fdiv_rn(mod, nrm);
+            v[m] = make_float2(__fmul_rn(v[m].x, f), __fmul_rn(v[m].y, f));
+        }
+        reg_fft_1buf<N, ColSwz<N, NB>, +1>(v, sX, b, l, J.pcol.tw);
+        if (ok) {
+#pragma unroll
+            for (int m = 0; m < 8; ++m) J.X[(size_t)(l + m * Q) * W + x] = v[m];
+        }
+        fence_proxy_async_smem();
+        __syncthreads();
+        item = nxt;
     }
 }
 

@@ -31,7 +31,8 @@ typedef enum imr_status {
     IMR_ERR_OUT_OF_MEMORY = 3,     /* device or host allocation failed        */
     IMR_ERR_CUDA = 4,              /* a CUDA runtime call failed              */
     IMR_ERR_NOT_INITIALIZED = 5,   /* task queue used before imr_queue_init   */
-    IMR_ERR_QUEUE = 6              /* task queue / serving loop failure       */
+    IMR_ERR_QUEUE = 6,             /* task queue / serving loop failure       */
+    IMR_ERR_DEVICE_TIMEOUT = 7     /* a bounded device-side wait gave up      */
 } imr_status;
 
 /* Parameters of one reconstruction, same meaning as the reference's
