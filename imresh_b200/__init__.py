@@ -262,3 +262,101 @@ def vector_max(d_data, n: int, stream=None) -> float:
     r = C.c_float()
     _check(lib().imr_vector_max(_ptr(d_data), n, C.byref(r), _stream(stream)), "imr_vector_max")
     return r.value
+
+
+# ------------------------------------------------------------------ engine
+class CResult(C.Structure):
+    _fields_ = [("tag", C.c_longlong), ("width", C.c_uint), ("height", C.c_uint),
+                ("cycles_done", C.c_int), ("last_error", C.c_float), ("latency_ms", C.c_double),
+                ("status", C.c_int)]
+
+
+class CEngineInfo(C.Structure):
+    _fields_ = [("pending", C.c_int), ("active", C.c_int), ("done", C.c_int),
+                ("device_bytes_used", C.c_size_t), ("device_bytes_peak", C.c_size_t),
+                ("device_bytes_budget", C.c_size_t), ("launches", C.c_long), ("steps", C.c_long)]
+
+
+def _engine_sigs(L):
+    vp = C.c_void_p
+    L.imr_engine_create.argtypes = [C.POINTER(vp), C.c_size_t, C.c_int, vp]
+    L.imr_engine_submit.argtypes = [vp, vp, vp, C.c_uint, C.c_uint, C.POINTER(CParams), C.c_longlong]
+    L.imr_engine_step.argtypes = [vp]
+    L.imr_engine_run.argtypes = [vp]
+    L.imr_engine_poll.argtypes = [vp, C.POINTER(CResult), C.c_int, C.POINTER(C.c_int)]
+    L.imr_engine_stats.argtypes = [vp, C.POINTER(CEngineInfo)]
+    L.imr_engine_destroy.argtypes = [vp]
+    L.imr_diffraction_intensity.argtypes = [vp, C.c_uint, C.c_uint, vp]
+
+
+class Engine:
+    """Batched, continuously-admitting engine (imr_engine_*).
+
+    submit() queues a host modulus and a host output buffer (both kept alive
+    here until the result is polled); step() runs one shrink-wrap cycle of
+    every active reconstruction; poll() returns finished results."""
+
+    def __init__(self, device_bytes: int = 0, max_jobs: int = 4096, stream=None):
+        L = lib()
+        _engine_sigs(L)
+        h = C.c_void_p()
+        _check(L.imr_engine_create(C.byref(h), device_bytes, max_jobs, _stream(stream)),
+               "imr_engine_create")
+        self._h = h
+        self._keep = {}
+
+    def submit(self, modulus: np.ndarray, params: Params | None = None, tag: int = 0,
+               out: np.ndarray | None = None) -> np.ndarray:
+        m = np.ascontiguousarray(modulus, dtype=np.float32)
+        H, W = m.shape
+        if out is None:
+            out = np.empty_like(m)
+        cp = (params or Params()).c()
+        _check(lib().imr_engine_submit(self._h, m.ctypes.data, out.ctypes.data, W, H,
+                                       C.byref(cp), tag), "imr_engine_submit")
+        self._keep[tag] = (m, out)
+        return out
+
+    def step(self):
+        _check(lib().imr_engine_step(self._h), "imr_engine_step")
+
+    def run(self):
+        _check(lib().imr_engine_run(self._h), "imr_engine_run")
+
+    def poll(self, max_results: int = 4096):
+        res = (CResult * max_results)()
+        n = C.c_int()
+        _check(lib().imr_engine_poll(self._h, res, max_results, C.byref(n)), "imr_engine_poll")
+        out = []
+        for r in res[:n.value]:
+            m, o = self._keep.pop(r.tag, (None, None))
+            out.append(dict(tag=r.tag, width=r.width, height=r.height, cycles_done=r.cycles_done,
+                            last_error=r.last_error, latency_ms=r.latency_ms, status=r.status,
+                            out=o))
+        return out
+
+    def info(self) -> dict:
+        i = CEngineInfo()
+        _check(lib().imr_engine_stats(self._h, C.byref(i)), "imr_engine_stats")
+        return {k: getattr(i, k) for k, _ in CEngineInfo._fields_}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().imr_engine_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def diffraction_intensity(obj: np.ndarray) -> np.ndarray:
+    """|FFT2(obj)| of a real float32 image on the engine's FFT (host in/out)."""
+    L = lib()
+    _engine_sigs(L)
+    a = np.ascontiguousarray(obj, dtype=np.float32).copy()
+    H, W = a.shape
+    _check(L.imr_diffraction_intensity(a.ctypes.data, W, H, _stream(None)), "imr_diffraction_intensity")
+    return a

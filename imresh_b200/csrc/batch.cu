@@ -1,0 +1,444 @@
+// Batched, continuously-admitting reconstruction engine (the served form of
+// the path) and its C ABI.
+//
+// The reference runs one cudaShrinkWrap per request on one of three CUDA
+// streams, from a std::thread per task (src/imresh/io/taskQueue.cu:91-193);
+// every cycle synchronises the host twice and allocates and frees device
+// memory.  Here all admitted reconstructions live on the device at once and
+// advance together: one step runs one shrink-wrap cycle of every active
+// reconstruction, with every pass of the cycle launched once per image-side
+// class (rows grouped by width, columns by height) over a device-resident
+// work list that covers all reconstructions of that class.  Reconstructions
+// of different sizes therefore share every launch of their class; new
+// requests are admitted between steps as device memory frees up, finished
+// ones (stop test met or cycles exhausted, decided on the device) retire and
+// their results are copied out.
+#include <cuda_runtime.h>
+#include <string.h>
+
+#include <algorithm>
+#include <chrono>
+#include <deque>
+#include <map>
+#include <vector>
+
+#include "imresh_b200.h"
+#include "kernels.cuh"
+#include "engine_host.hpp"
+
+namespace imr {
+
+static double now_ms()
+{
+    using namespace std::chrono;
+    return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+struct EJob {
+    int slot = -1;
+    unsigned W = 0, H = 0;
+    imr_params p{};
+    const float *h_in = nullptr;
+    float *h_out = nullptr;
+    long long tag = 0;
+    double t_submit = 0, t_done = 0;
+    char *arena = nullptr;
+    JobDev J{};
+    JobShape S;
+    int cycles_done = 0;
+    float last_error = 0.f;
+    int status = IMR_SUCCESS;
+};
+
+// kernels + list slice of one launch group
+struct Group {
+    int key_n = 0;            // image side of the class
+    bool pipelined = false;
+    RowKernels rk{};
+    ColKernels ck{};
+    size_t smem = 0, smem_fin = 0;
+    std::vector<WorkItem> items;   // sorted by job n_hio, descending
+    std::vector<int> hio_count;    // items whose job runs iteration i
+    int list_base = 0;             // index of this group's first WorkList header
+};
+
+}  // namespace imr
+
+using namespace imr;
+
+struct imr_engine {
+    int dev = 0;
+    cudaStream_t s = nullptr;
+    size_t budget = 0, used = 0, peak = 0;
+    int max_slots = 0;
+    JobDev *dj = nullptr;           // [max_slots]
+    JobState *dst = nullptr;        // [max_slots]
+    JobState *hst = nullptr;        // pinned mirror
+    std::vector<int> free_slots;
+    std::deque<EJob *> pending;
+    std::vector<EJob *> active;
+    std::vector<EJob *> done;
+    WorkItem *d_items = nullptr;
+    size_t items_cap = 0;
+    WorkList *d_lists = nullptr;
+    size_t lists_cap = 0;
+    WorkItem *h_items = nullptr;   // pinned staging
+    WorkList *h_lists = nullptr;
+    long launches = 0;
+    long steps = 0;
+    int sms = 148;
+};
+
+#define CKE(call)                      \
+    do {                               \
+        cudaError_t e_ = (call);       \
+        if (e_ != cudaSuccess) {       \
+            set_error(#call, e_);      \
+            return IMR_ERR_CUDA;       \
+        }                              \
+    } while (0)
+
+static int grow(imr_engine *E, size_t n_items, size_t n_lists)
+{
+    if (n_items > E->items_cap) {
+        size_t cap = std::max(n_items, E->items_cap * 2 + 1024);
+        if (E->d_items) cudaFree(E->d_items);
+        if (E->h_items) cudaFreeHost(E->h_items);
+        CKE(cudaMalloc(&E->d_items, cap * sizeof(WorkItem)));
+        CKE(cudaMallocHost(&E->h_items, cap * sizeof(WorkItem)));
+        E->items_cap = cap;
+    }
+    if (n_lists > E->lists_cap) {
+        size_t cap = std::max(n_lists, E->lists_cap * 2 + 256);
+        if (E->d_lists) cudaFree(E->d_lists);
+        if (E->h_lists) cudaFreeHost(E->h_lists);
+        CKE(cudaMalloc(&E->d_lists, cap * sizeof(WorkList)));
+        CKE(cudaMallocHost(&E->h_lists, cap * sizeof(WorkList)));
+        E->lists_cap = cap;
+    }
+    return IMR_SUCCESS;
+}
+
+// Loop-kernel grid: enough CTAs to fill the GPU, never more than the items.
+static int loop_grid(const imr_engine *E, int items) { return std::max(1, std::min(items, E->sms * 16)); }
+
+static int admit(imr_engine *E, std::vector<EJob *> &fresh)
+{
+    while (!E->pending.empty() && !E->free_slots.empty()) {
+        EJob *j = E->pending.front();
+        if (E->used + j->S.bytes > E->budget && !(E->active.empty() && fresh.empty())) break;
+        E->pending.pop_front();
+        j->slot = E->free_slots.back();
+        E->free_slots.pop_back();
+        cudaError_t e = cudaMallocAsync((void **)&j->arena, j->S.bytes, E->s);
+        if (e != cudaSuccess) {   // allocation failed: back to the queue, retry later
+            E->free_slots.push_back(j->slot);
+            j->slot = -1;
+            E->pending.push_front(j);
+            cudaGetLastError();
+            break;
+        }
+        E->used += j->S.bytes;
+        E->peak = std::max(E->peak, E->used);
+        job_bind(j->J, j->S, j->arena, E->dst + j->slot);
+        int rc = job_upload(j->J, j->S, j->arena, E->dj + j->slot, E->s);
+        if (rc) return rc;
+        CKE(cudaMemsetAsync(E->dst + j->slot, 0, sizeof(JobState), E->s));
+        CKE(cudaMemcpyAsync((void *)j->J.M, j->h_in, (size_t)j->W * j->H * 4, cudaMemcpyHostToDevice, E->s));
+        E->active.push_back(j);
+        fresh.push_back(j);
+    }
+    return IMR_SUCCESS;
+}
+
+// Group jobs by the row kernels (width) or the column kernels (height and
+// pipelining), items sorted by the job's HIO count so iteration i runs a
+// prefix of the list.
+static void build_groups(const std::vector<EJob *> &jobs, bool rows, std::vector<Group> &out)
+{
+    std::map<std::pair<int, int>, std::vector<EJob *>> by;
+    for (EJob *j : jobs) {
+        const int key = rows ? (int)j->W : (int)j->H;
+        const int pl = rows ? (j->S.p_rows ? 1 : 0) : (j->S.p_cols ? 1 : 0);
+        by[{key, pl}].push_back(j);
+    }
+    out.clear();
+    for (auto &kv : by) {
+        Group g;
+        g.key_n = kv.first.first;
+        g.pipelined = kv.first.second != 0;
+        auto &v = kv.second;
+        std::stable_sort(v.begin(), v.end(), [](EJob *a, EJob *b) { return a->J.n_hio > b->J.n_hio; });
+        const EJob *j0 = v.front();
+        g.rk = j0->S.rk;
+        g.ck = j0->S.ck;
+        g.smem = rows ? j0->S.smem_row : j0->S.smem_col;
+        g.smem_fin = j0->S.smem_fin;
+        int max_hio = 0;
+        for (EJob *j : v) {
+            const int nt = rows ? j->J.n_row_tiles : j->J.n_col_tiles;
+            for (int t = 0; t < nt; ++t) g.items.push_back(WorkItem{j->slot, t});
+            max_hio = std::max(max_hio, j->J.n_hio);
+        }
+        g.hio_count.assign(max_hio, 0);
+        for (EJob *j : v) {
+            const int nt = rows ? j->J.n_row_tiles : j->J.n_col_tiles;
+            for (int i = 0; i < j->J.n_hio; ++i) g.hio_count[i] += nt;
+        }
+        out.push_back(std::move(g));
+    }
+}
+
+static int launch_step(imr_engine *E, const std::vector<EJob *> &fresh)
+{
+    cudaStream_t s = E->s;
+    // --- column init of newly admitted jobs
+    std::vector<Group> init_groups, rowg, colg;
+    build_groups(fresh, false, init_groups);
+    std::vector<EJob *> live;
+    for (EJob *j : E->active) live.push_back(j);
+    build_groups(live, true, rowg);
+    build_groups(live, false, colg);
+    // vertical-blur items: every live job
+    std::vector<WorkItem> vb;
+    for (EJob *j : live)
+        for (int t = 0; t < j->J.n_vb_tiles; ++t) vb.push_back(WorkItem{j->slot, t});
+
+    size_t n_items = vb.size(), n_lists = 1;
+    for (auto *G : {&init_groups, &rowg, &colg})
+        for (auto &g : *G) {
+            n_items += g.items.size();
+            n_lists += 1 + g.hio_count.size();
+        }
+    int rc = grow(E, n_items, n_lists);
+    if (rc) return rc;
+    size_t ip = 0, lp = 0;
+    auto put = [&](const std::vector<WorkItem> &items, const std::vector<int> &counts, int &base) {
+        const WorkItem *dptr = E->d_items + ip;
+        memcpy(E->h_items + ip, items.data(), items.size() * sizeof(WorkItem));
+        base = (int)lp;
+        E->h_lists[lp++] = WorkList{dptr, (int)items.size()};
+        for (int c : counts) E->h_lists[lp++] = WorkList{dptr, c};
+        ip += items.size();
+    };
+    int vb_base = 0;
+    put(vb, {}, vb_base);
+    for (auto *G : {&init_groups, &rowg, &colg})
+        for (auto &g : *G) put(g.items, g.hio_count, g.list_base);
+    CKE(cudaMemcpyAsync(E->d_items, E->h_items, ip * sizeof(WorkItem), cudaMemcpyHostToDevice, s));
+    CKE(cudaMemcpyAsync(E->d_lists, E->h_lists, lp * sizeof(WorkList), cudaMemcpyHostToDevice, s));
+    const WorkList *L = E->d_lists;
+
+    for (auto &g : init_groups) {
+        g.ck.init<<<loop_grid(E, (int)g.items.size()), g.ck.threads, g.ck.smem ? g.ck.smem : g.smem, s>>>(
+            E->dj, L + g.list_base);
+        ++E->launches;
+    }
+    // --- one shrink-wrap cycle of every live job
+    for (auto &g : rowg) {
+        g.rk.finish<<<loop_grid(E, (int)g.items.size()), g.rk.threads, g.smem_fin, s>>>(E->dj, L + g.list_base,
+                                                                                     nullptr);
+        ++E->launches;
+    }
+    if (!vb.empty()) {
+        k_vblur<<<loop_grid(E, (int)vb.size()), kVbThreads, 0, s>>>(E->dj, L + vb_base);
+        ++E->launches;
+    }
+    int max_hio = 0;
+    for (auto &g : rowg) max_hio = std::max(max_hio, (int)g.hio_count.size());
+    for (int i = 0; i < max_hio; ++i) {
+        for (auto &g : rowg) {
+            if (i >= (int)g.hio_count.size()) continue;
+            const WorkList *Li = L + g.list_base + 1 + i;
+            const int n = g.hio_count[i];
+            if (g.pipelined) {
+                auto k = i == 0 ? g.rk.p_hio_first : g.rk.p_hio;
+                const int sm = i == 0 ? g.rk.p_smem_first : g.rk.p_smem;
+                k<<<persistent_grid((const void *)k, g.rk.threads, sm, n), g.rk.threads, sm, s>>>(E->dj, Li);
+            } else {
+                (i == 0 ? g.rk.hio_first : g.rk.hio)<<<loop_grid(E, n), g.rk.threads, g.smem, s>>>(E->dj, Li);
+            }
+            ++E->launches;
+        }
+        for (auto &g : colg) {
+            if (i >= (int)g.hio_count.size()) continue;
+            const WorkList *Li = L + g.list_base + 1 + i;
+            const int n = g.hio_count[i];
+            if (g.pipelined)
+                g.ck.p_col<<<persistent_grid((const void *)g.ck.p_col, g.ck.threads, g.ck.p_smem, n), g.ck.threads,
+                             g.ck.p_smem, s>>>(E->dj, Li);
+            else
+                g.ck.col<<<loop_grid(E, n), g.ck.threads, g.smem, s>>>(E->dj, Li);
+            ++E->launches;
+        }
+    }
+    CKE(cudaGetLastError());
+    return IMR_SUCCESS;
+}
+
+static int retire(imr_engine *E)
+{
+    CKE(cudaMemcpyAsync(E->hst, E->dst, sizeof(JobState) * E->max_slots, cudaMemcpyDeviceToHost, E->s));
+    CKE(cudaStreamSynchronize(E->s));
+    std::vector<EJob *> keep, out;
+    for (EJob *j : E->active) {
+        const JobState &st = E->hst[j->slot];
+        if (st.stop || st.err) {
+            j->cycles_done = st.cycles_done;
+            j->last_error = st.last_error;
+            j->status = st.err ? IMR_ERR_DEVICE_TIMEOUT : IMR_SUCCESS;
+            CKE(cudaMemcpyAsync(j->h_out, j->J.out, (size_t)j->W * j->H * 4, cudaMemcpyDeviceToHost, E->s));
+            CKE(cudaFreeAsync(j->arena, E->s));
+            out.push_back(j);
+        } else {
+            keep.push_back(j);
+        }
+    }
+    E->active.swap(keep);
+    if (!out.empty()) {
+        CKE(cudaStreamSynchronize(E->s));
+        const double t = now_ms();
+        for (EJob *j : out) {
+            j->t_done = t;
+            E->used -= j->S.bytes;
+            E->free_slots.push_back(j->slot);
+            j->arena = nullptr;
+            E->done.push_back(j);
+        }
+    }
+    return IMR_SUCCESS;
+}
+
+extern "C" {
+
+int imr_engine_create(imr_engine **out, size_t device_bytes, int max_jobs, void *stream)
+{
+    if (!out || max_jobs < 1) return IMR_ERR_INVALID_VALUE;
+    *out = nullptr;
+    int rc = ensure_kernel_attributes();
+    if (rc) return rc;
+    imr_engine *E = new imr_engine();
+    cudaGetDevice(&E->dev);
+    cudaDeviceGetAttribute(&E->sms, cudaDevAttrMultiProcessorCount, E->dev);
+    E->s = (cudaStream_t)stream;
+    if (device_bytes == 0) {
+        size_t fr = 0, tot = 0;
+        cudaMemGetInfo(&fr, &tot);
+        device_bytes = fr / 10 * 8;
+    }
+    E->budget = device_bytes;
+    E->max_slots = max_jobs;
+    cudaError_t e = cudaMalloc(&E->dj, sizeof(JobDev) * max_jobs);
+    if (e == cudaSuccess) e = cudaMalloc(&E->dst, sizeof(JobState) * max_jobs);
+    if (e == cudaSuccess) e = cudaMallocHost(&E->hst, sizeof(JobState) * max_jobs);
+    if (e == cudaSuccess) e = cudaMemset(E->dst, 0, sizeof(JobState) * max_jobs);
+    if (e != cudaSuccess) {
+        set_error("engine create", e);
+        imr_engine_destroy(E);
+        return IMR_ERR_OUT_OF_MEMORY;
+    }
+    for (int i = max_jobs - 1; i >= 0; --i) E->free_slots.push_back(i);
+    *out = E;
+    return IMR_SUCCESS;
+}
+
+int imr_engine_submit(imr_engine *E, const float *h_modulus, float *h_out, unsigned W, unsigned H,
+                      const imr_params *params, long long tag)
+{
+    if (!E || !h_modulus || !h_out || W == 0 || H == 0) return IMR_ERR_INVALID_VALUE;
+    EJob *j = new EJob();
+    j->W = W;
+    j->H = H;
+    resolve_params(params, j->p);
+    int rc = job_prepare(W, H, j->p, j->J, j->S);
+    if (rc) {
+        delete j;
+        return rc;
+    }
+    j->h_in = h_modulus;
+    j->h_out = h_out;
+    j->tag = tag;
+    j->t_submit = now_ms();
+    E->pending.push_back(j);
+    return IMR_SUCCESS;
+}
+
+int imr_engine_step(imr_engine *E)
+{
+    if (!E) return IMR_ERR_INVALID_VALUE;
+    std::vector<EJob *> fresh;
+    int rc = admit(E, fresh);
+    if (rc) return rc;
+    if (E->active.empty()) return IMR_SUCCESS;
+    if ((rc = launch_step(E, fresh))) return rc;
+    ++E->steps;
+    return retire(E);
+}
+
+int imr_engine_poll(imr_engine *E, imr_result *results, int max_results, int *n_results)
+{
+    if (!E || !n_results || (max_results > 0 && !results)) return IMR_ERR_INVALID_VALUE;
+    int n = 0;
+    while (n < max_results && !E->done.empty()) {
+        EJob *j = E->done.front();
+        E->done.erase(E->done.begin());
+        imr_result &r = results[n++];
+        r.tag = j->tag;
+        r.width = j->W;
+        r.height = j->H;
+        r.cycles_done = j->cycles_done;
+        r.last_error = j->last_error;
+        r.latency_ms = j->t_done - j->t_submit;
+        r.status = j->status;
+        delete j;
+    }
+    *n_results = n;
+    return IMR_SUCCESS;
+}
+
+int imr_engine_run(imr_engine *E)
+{
+    if (!E) return IMR_ERR_INVALID_VALUE;
+    while (!E->pending.empty() || !E->active.empty()) {
+        int rc = imr_engine_step(E);
+        if (rc) return rc;
+    }
+    return IMR_SUCCESS;
+}
+
+int imr_engine_stats(imr_engine *E, imr_engine_info *st)
+{
+    if (!E || !st) return IMR_ERR_INVALID_VALUE;
+    st->pending = (int)E->pending.size();
+    st->active = (int)E->active.size();
+    st->done = (int)E->done.size();
+    st->device_bytes_used = E->used;
+    st->device_bytes_peak = E->peak;
+    st->device_bytes_budget = E->budget;
+    st->launches = E->launches;
+    st->steps = E->steps;
+    return IMR_SUCCESS;
+}
+
+int imr_engine_destroy(imr_engine *E)
+{
+    if (!E) return IMR_SUCCESS;
+    cudaStreamSynchronize(E->s);
+    for (EJob *j : E->active) {
+        if (j->arena) cudaFree(j->arena);
+        delete j;
+    }
+    for (EJob *j : E->pending) delete j;
+    for (EJob *j : E->done) delete j;
+    if (E->dj) cudaFree(E->dj);
+    if (E->dst) cudaFree(E->dst);
+    if (E->hst) cudaFreeHost(E->hst);
+    if (E->d_items) cudaFree(E->d_items);
+    if (E->h_items) cudaFreeHost(E->h_items);
+    if (E->d_lists) cudaFree(E->d_lists);
+    if (E->h_lists) cudaFreeHost(E->h_lists);
+    delete E;
+    return IMR_SUCCESS;
+}
+
+}  // extern "C"

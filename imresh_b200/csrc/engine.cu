@@ -8,6 +8,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <map>
 #include <mutex>
 #include <vector>
@@ -315,6 +316,7 @@ struct imr_plan {
     ColKernels ck{};
     bool p_rows = false, p_cols = false;   // pipelined passes in use
     int g_row_first = 0, g_row = 0, g_col = 0;
+    WorkList *Lrow = nullptr, *Lcol = nullptr, *Lvb = nullptr;   // device
 };
 
 static int plan_launch_cycle(imr_plan *P, cudaStream_t s)
@@ -322,21 +324,21 @@ static int plan_launch_cycle(imr_plan *P, cudaStream_t s)
     const JobDev &J = P->hj;
     const RowKernels &rk = P->rk;
     const ColKernels &ck = P->ck;
-    rk.finish<<<J.n_row_tiles, rk.threads, P->smem_fin, s>>>(P->dj, nullptr, P->dbg_gprime);
-    k_vblur<<<J.n_vb_tiles, kVbThreads, 0, s>>>(P->dj, nullptr);
+    rk.finish<<<J.n_row_tiles, rk.threads, P->smem_fin, s>>>(P->dj, P->Lrow, P->dbg_gprime);
+    k_vblur<<<J.n_vb_tiles, kVbThreads, 0, s>>>(P->dj, P->Lvb);
     for (int i = 0; i < J.n_hio; ++i) {
         if (P->p_rows) {
             if (i == 0)
-                rk.p_hio_first<<<P->g_row_first, rk.threads, rk.p_smem_first, s>>>(P->dj, nullptr, J.n_row_tiles);
+                rk.p_hio_first<<<P->g_row_first, rk.threads, rk.p_smem_first, s>>>(P->dj, P->Lrow);
             else
-                rk.p_hio<<<P->g_row, rk.threads, rk.p_smem, s>>>(P->dj, nullptr, J.n_row_tiles);
+                rk.p_hio<<<P->g_row, rk.threads, rk.p_smem, s>>>(P->dj, P->Lrow);
         } else {
-            (i == 0 ? rk.hio_first : rk.hio)<<<J.n_row_tiles, rk.threads, P->smem_row, s>>>(P->dj, nullptr);
+            (i == 0 ? rk.hio_first : rk.hio)<<<J.n_row_tiles, rk.threads, P->smem_row, s>>>(P->dj, P->Lrow);
         }
         if (P->p_cols)
-            ck.p_col<<<P->g_col, ck.threads, ck.p_smem, s>>>(P->dj, nullptr, J.n_col_tiles);
+            ck.p_col<<<P->g_col, ck.threads, ck.p_smem, s>>>(P->dj, P->Lcol);
         else
-            ck.col<<<J.n_col_tiles, ck.threads, P->smem_col, s>>>(P->dj, nullptr);
+            ck.col<<<J.n_col_tiles, ck.threads, P->smem_col, s>>>(P->dj, P->Lcol);
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
@@ -354,6 +356,106 @@ static int plan_launch_cycle(imr_plan *P, cudaStream_t s)
             return IMR_ERR_CUDA;                  \
         }                                         \
     } while (0)
+
+namespace imr {
+
+// ---------------------------------------------------------------- one job
+// Host description of one reconstruction's device layout (shared by plans
+// and the batched engine).  Arena layout, 256-byte aligned pieces:
+// X, G (c64) | M, hb, vb, out (f32) | mask (u8) | weights | taps | error
+// partials | per-cycle errors.  The JobState lives wherever the caller puts
+// it (plans: after the arena; the engine: in one array for all jobs).
+int job_prepare(unsigned W, unsigned H, const imr_params &p, JobDev &J, JobShape &S)
+{
+    int rc;
+    memset(&J, 0, sizeof(J));
+    J.W = (int)W;
+    J.H = (int)H;
+    if ((rc = make_fft_plan((int)W, J.prow)) || (rc = make_fft_plan((int)H, J.pcol))) return rc;
+    if ((rc = build_weight_table(p, S.wt, S.taps))) return rc;
+    S.rk = row_kernels(J.W);
+    S.ck = col_kernels(J.H);
+    J.rpc = S.rk.nb < J.H ? S.rk.nb : J.H;
+    J.cpc = S.ck.nb < J.W ? S.ck.nb : J.W;
+    S.p_rows = S.rk.p_hio != nullptr;
+    S.p_cols = S.ck.p_col != nullptr && J.W % 4 == 0 && J.W >= S.ck.nb;
+    if (S.p_cols) J.cpc = S.ck.nb;
+    J.n_row_tiles = (J.H + J.rpc - 1) / J.rpc;
+    J.n_col_tiles = (J.W + J.cpc - 1) / J.cpc;
+    J.vb_tiles_x = (J.W + kVbTileX - 1) / kVbTileX;
+    J.n_vb_tiles = J.vb_tiles_x * ((J.H + kVbTileY - 1) / kVbTileY);
+    J.beta = p.hioBeta;
+    J.cut_auto = p.intensityCutOffAutoCorel;
+    J.cut = p.intensityCutOff;
+    J.target = p.targetError;
+    J.n_cycles = (int)p.nCycles;
+    J.n_hio = (int)p.nHioCycles;
+    // shared memory sized for the compile-time tile (NB sequences), even when
+    // the image has fewer rows / columns than NB
+    if (S.rk.smem) {
+        S.smem_row = S.smem_fin = (size_t)S.rk.smem;   // norms reuse the FFT buffers
+    } else {
+        S.smem_row = (size_t)S.rk.nb * J.W * sizeof(float2);
+        S.smem_fin = S.smem_row + (size_t)S.rk.nb * J.W * sizeof(float);
+    }
+    S.smem_col = S.ck.smem ? (size_t)S.ck.smem : (size_t)S.ck.nb * J.H * sizeof(float2);
+    const size_t N = (size_t)W * H;
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    size_t off = 0;
+    S.oX = off; off += al(N * 8);
+    S.oG = off; off += al(N * 8);
+    S.oM = off; off += al(N * 4);
+    S.oHB = off; off += al(N * 4);
+    S.oVB = off; off += al(N * 4);
+    S.oOut = off; off += al(N * 4);
+    S.oMask = off; off += al(N);
+    S.oW = off; off += al(S.wt.size() * 4);
+    S.oT = off; off += al(S.taps.size() * 4);
+    S.oEP = off; off += al((size_t)2 * J.n_row_tiles * 8);
+    S.oErr = off; off += al((size_t)(J.n_cycles + 1) * 4);
+    S.bytes = off;
+    return IMR_SUCCESS;
+}
+
+void job_bind(JobDev &J, JobShape &S, char *a, JobState *st)
+{
+    J.X = (float2 *)(a + S.oX);
+    J.G = (float2 *)(a + S.oG);
+    J.M = (const float *)(a + S.oM);
+    J.hb = (float *)(a + S.oHB);
+    J.vb = (float *)(a + S.oVB);
+    J.out = (float *)(a + S.oOut);
+    J.mask = (uint8_t *)(a + S.oMask);
+    J.weights = (const float *)(a + S.oW);
+    J.ntaps = (const int *)(a + S.oT);
+    J.err_part = (double *)(a + S.oEP);
+    J.errors = (float *)(a + S.oErr);
+    J.st = st;
+    J.use_tma_cols = 0;
+    if (S.p_cols) {
+        const int br = S.ck.p_box_rows;
+        bool okm = encode_tensor_map(&J.tmX, J.X, J.W, J.H, 8, S.ck.nb, br);
+        if (okm && S.ck.p_tma_m) okm = encode_tensor_map(&J.tmM, J.M, J.W, J.H, 4, S.ck.nb, br);
+        if (!okm) {   // shape the TMA unit cannot describe: per-tile column pass
+            S.p_cols = false;
+            J.cpc = S.ck.nb < J.W ? S.ck.nb : J.W;
+            J.n_col_tiles = (J.W + J.cpc - 1) / J.cpc;
+        }
+        J.use_tma_cols = S.p_cols ? 1 : 0;
+    }
+}
+
+int job_upload(const JobDev &J, const JobShape &S, char *a, JobDev *dj, cudaStream_t s)
+{
+    const size_t N = (size_t)J.W * J.H;
+    CK(cudaMemcpyAsync(a + S.oW, S.wt.data(), S.wt.size() * 4, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(a + S.oT, S.taps.data(), S.taps.size() * 4, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(dj, &J, sizeof(JobDev), cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(a + S.oMask, 0, N, s));
+    CK(cudaMemsetAsync(a + S.oErr, 0, (size_t)(J.n_cycles + 1) * 4, s));
+    return IMR_SUCCESS;
+}
+}  // namespace imr
 
 extern "C" {
 
@@ -411,44 +513,35 @@ int imr_plan_create(imr_plan **out, unsigned W, unsigned H, const imr_params *pa
     P->H = (int)H;
     resolve_params(params, P->p);
     JobDev &J = P->hj;
-    J.W = (int)W;
-    J.H = (int)H;
-    if ((rc = make_fft_plan((int)W, J.prow)) || (rc = make_fft_plan((int)H, J.pcol))) {
+    JobShape S;
+    if ((rc = job_prepare(W, H, P->p, J, S))) {
         delete P;
         return rc;
     }
-    std::vector<float> wt;
-    std::vector<int> taps;
-    if ((rc = build_weight_table(P->p, wt, taps))) {
+    const size_t extra = (sizeof(JobState) + 255) / 256 * 256 + (sizeof(JobDev) + 255) / 256 * 256 +
+                         (3 * sizeof(WorkList) + 255) / 256 * 256;
+    cudaError_t e = cudaMalloc(&P->arena, S.bytes + extra);
+    if (e != cudaSuccess) {
+        set_error("cudaMalloc plan arena", e);
         delete P;
-        return rc;
+        return IMR_ERR_OUT_OF_MEMORY;
     }
-    P->rk = row_kernels(J.W);
-    P->ck = col_kernels(J.H);
-    J.rpc = P->rk.nb < J.H ? P->rk.nb : J.H;
-    J.cpc = P->ck.nb < J.W ? P->ck.nb : J.W;
-    P->p_rows = P->rk.p_hio != nullptr;
-    P->p_cols = P->ck.p_col != nullptr && J.W % 4 == 0 && J.W >= P->ck.nb;
-    if (P->p_cols) J.cpc = P->ck.nb;
-    J.n_row_tiles = (J.H + J.rpc - 1) / J.rpc;
-    J.n_col_tiles = (J.W + J.cpc - 1) / J.cpc;
-    J.vb_tiles_x = (J.W + kVbTileX - 1) / kVbTileX;
-    J.n_vb_tiles = J.vb_tiles_x * ((J.H + kVbTileY - 1) / kVbTileY);
-    J.beta = P->p.hioBeta;
-    J.cut_auto = P->p.intensityCutOffAutoCorel;
-    J.cut = P->p.intensityCutOff;
-    J.target = P->p.targetError;
-    J.n_cycles = (int)P->p.nCycles;
-    J.n_hio = (int)P->p.nHioCycles;
-    // shared memory sized for the compile-time tile (NB sequences), even when
-    // the image has fewer rows / columns than NB
-    if (P->rk.smem) {
-        P->smem_row = P->smem_fin = (size_t)P->rk.smem;   // norms reuse the FFT buffers
-    } else {
-        P->smem_row = (size_t)P->rk.nb * J.W * sizeof(float2);
-        P->smem_fin = P->smem_row + (size_t)P->rk.nb * J.W * sizeof(float);
-    }
-    P->smem_col = P->ck.smem ? (size_t)P->ck.smem : (size_t)P->ck.nb * J.H * sizeof(float2);
+    char *a = (char *)P->arena;
+    char *tail = a + S.bytes;
+    JobState *st = (JobState *)tail;
+    P->dj = (JobDev *)(tail + (sizeof(JobState) + 255) / 256 * 256);
+    P->Lrow = (WorkList *)((char *)P->dj + (sizeof(JobDev) + 255) / 256 * 256);
+    P->Lcol = P->Lrow + 1;
+    P->Lvb = P->Lrow + 2;
+    job_bind(J, S, a, st);
+    P->st = J.st;
+    P->rk = S.rk;
+    P->ck = S.ck;
+    P->p_rows = S.p_rows;
+    P->p_cols = S.p_cols;
+    P->smem_row = S.smem_row;
+    P->smem_fin = S.smem_fin;
+    P->smem_col = S.smem_col;
     if (P->p_rows) {
         P->g_row_first = persistent_grid((const void *)P->rk.p_hio_first, P->rk.threads, P->rk.p_smem_first,
                                          J.n_row_tiles);
@@ -456,61 +549,10 @@ int imr_plan_create(imr_plan **out, unsigned W, unsigned H, const imr_params *pa
     }
     if (P->p_cols)
         P->g_col = persistent_grid((const void *)P->ck.p_col, P->ck.threads, P->ck.p_smem, J.n_col_tiles);
-
-    // one arena: X, G (c64), M, hb, vb, out (f32), mask (u8), tables, state
-    const size_t N = (size_t)W * H;
-    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
-    size_t off = 0;
-    const size_t oX = off; off += al(N * 8);
-    const size_t oG = off; off += al(N * 8);
-    const size_t oM = off; off += al(N * 4);
-    const size_t oHB = off; off += al(N * 4);
-    const size_t oVB = off; off += al(N * 4);
-    const size_t oOut = off; off += al(N * 4);
-    const size_t oMask = off; off += al(N);
-    const size_t oW = off; off += al(wt.size() * 4);
-    const size_t oT = off; off += al(taps.size() * 4);
-    const size_t oEP = off; off += al((size_t)2 * J.n_row_tiles * 8);
-    const size_t oErr = off; off += al((size_t)(J.n_cycles + 1) * 4);
-    const size_t oSt = off; off += al(sizeof(JobState));
-    const size_t oJ = off; off += al(sizeof(JobDev));
-    cudaError_t e = cudaMalloc(&P->arena, off);
-    if (e != cudaSuccess) {
-        set_error("cudaMalloc plan arena", e);
-        delete P;
-        return IMR_ERR_OUT_OF_MEMORY;
-    }
-    char *a = (char *)P->arena;
-    J.X = (float2 *)(a + oX);
-    J.G = (float2 *)(a + oG);
-    J.M = (const float *)(a + oM);
-    J.hb = (float *)(a + oHB);
-    J.vb = (float *)(a + oVB);
-    J.out = (float *)(a + oOut);
-    J.mask = (uint8_t *)(a + oMask);
-    J.weights = (const float *)(a + oW);
-    J.ntaps = (const int *)(a + oT);
-    J.err_part = (double *)(a + oEP);
-    J.errors = (float *)(a + oErr);
-    J.st = (JobState *)(a + oSt);
-    P->st = J.st;
-    P->dj = (JobDev *)(a + oJ);
-    if (P->p_cols) {
-        const int br = P->ck.p_box_rows;
-        bool okm = encode_tensor_map(&J.tmX, J.X, J.W, J.H, 8, P->ck.nb, br);
-        if (okm && P->ck.p_tma_m) okm = encode_tensor_map(&J.tmM, J.M, J.W, J.H, 4, P->ck.nb, br);
-        if (!okm) {   // shape the TMA unit cannot describe: per-tile column pass
-            P->p_cols = false;
-            J.cpc = P->ck.nb < J.W ? P->ck.nb : J.W;
-            J.n_col_tiles = (J.W + J.cpc - 1) / J.cpc;
-        }
-        J.use_tma_cols = P->p_cols ? 1 : 0;
-    }
-    e = cudaMemcpy(a + oW, wt.data(), wt.size() * 4, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(a + oT, taps.data(), taps.size() * 4, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(P->dj, &J, sizeof(JobDev), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemset(a + oMask, 0, N);
-    if (e == cudaSuccess) e = cudaMemset(a + oErr, 0, (size_t)(J.n_cycles + 1) * 4);
+    const WorkList lists[3] = {{nullptr, J.n_row_tiles}, {nullptr, J.n_col_tiles}, {nullptr, J.n_vb_tiles}};
+    e = cudaMemcpy(P->Lrow, lists, sizeof(lists), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = job_upload(J, S, a, P->dj, 0) ? cudaErrorUnknown : cudaSuccess;
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
         set_error("plan upload", e);
         imr_plan_destroy(P);
@@ -553,11 +595,11 @@ int imr_plan_execute(imr_plan *P, const float *d_modulus, float *d_out, void *st
     const size_t N = (size_t)P->W * P->H;
     CK(cudaMemcpyAsync((void *)J.M, d_modulus, N * 4, cudaMemcpyDeviceToDevice, s));
     CK(cudaMemsetAsync(P->st, 0, sizeof(JobState), s));
-    P->ck.init<<<J.n_col_tiles, P->ck.threads, P->smem_col, s>>>(P->dj, nullptr);
+    P->ck.init<<<J.n_col_tiles, P->ck.threads, P->smem_col, s>>>(P->dj, P->Lcol);
     CK(cudaGetLastError());
     for (int c = 0; c < J.n_cycles; ++c) CK(cudaGraphLaunch(P->gexec, s));
-    P->rk.finish<<<J.n_row_tiles, P->rk.threads, P->smem_fin, s>>>(P->dj, nullptr, P->dbg_gprime);
-    k_vblur<<<J.n_vb_tiles, kVbThreads, 0, s>>>(P->dj, nullptr);
+    P->rk.finish<<<J.n_row_tiles, P->rk.threads, P->smem_fin, s>>>(P->dj, P->Lrow, P->dbg_gprime);
+    k_vblur<<<J.n_vb_tiles, kVbThreads, 0, s>>>(P->dj, P->Lvb);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(d_out, J.out, N * 4, cudaMemcpyDeviceToDevice, s));
     return IMR_SUCCESS;
@@ -571,11 +613,11 @@ int imr_plan_execute_host(imr_plan *P, const float *h_modulus, float *h_out, voi
     const size_t N = (size_t)P->W * P->H;
     CK(cudaMemcpyAsync((void *)J.M, h_modulus, N * 4, cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(P->st, 0, sizeof(JobState), s));
-    P->ck.init<<<J.n_col_tiles, P->ck.threads, P->smem_col, s>>>(P->dj, nullptr);
+    P->ck.init<<<J.n_col_tiles, P->ck.threads, P->smem_col, s>>>(P->dj, P->Lcol);
     CK(cudaGetLastError());
     for (int c = 0; c < J.n_cycles; ++c) CK(cudaGraphLaunch(P->gexec, s));
-    P->rk.finish<<<J.n_row_tiles, P->rk.threads, P->smem_fin, s>>>(P->dj, nullptr, P->dbg_gprime);
-    k_vblur<<<J.n_vb_tiles, kVbThreads, 0, s>>>(P->dj, nullptr);
+    P->rk.finish<<<J.n_row_tiles, P->rk.threads, P->smem_fin, s>>>(P->dj, P->Lrow, P->dbg_gprime);
+    k_vblur<<<J.n_vb_tiles, kVbThreads, 0, s>>>(P->dj, P->Lvb);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(h_out, J.out, N * 4, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
@@ -628,14 +670,14 @@ int imr_plan_profile(imr_plan *P, int iters, void *stream, float *ms_row, float 
     CK(cudaEventRecord(ev[0], s));
     for (int i = 0; i < iters; ++i) {
         if (P->p_rows)
-            P->rk.p_hio<<<P->g_row, P->rk.threads, P->rk.p_smem, s>>>(P->dj, nullptr, J.n_row_tiles);
+            P->rk.p_hio<<<P->g_row, P->rk.threads, P->rk.p_smem, s>>>(P->dj, P->Lrow);
         else
-            P->rk.hio<<<J.n_row_tiles, P->rk.threads, P->smem_row, s>>>(P->dj, nullptr);
+            P->rk.hio<<<J.n_row_tiles, P->rk.threads, P->smem_row, s>>>(P->dj, P->Lrow);
         CK(cudaEventRecord(ev[2 * i + 1], s));
         if (P->p_cols)
-            P->ck.p_col<<<P->g_col, P->ck.threads, P->ck.p_smem, s>>>(P->dj, nullptr, J.n_col_tiles);
+            P->ck.p_col<<<P->g_col, P->ck.threads, P->ck.p_smem, s>>>(P->dj, P->Lcol);
         else
-            P->ck.col<<<J.n_col_tiles, P->ck.threads, P->smem_col, s>>>(P->dj, nullptr);
+            P->ck.col<<<J.n_col_tiles, P->ck.threads, P->smem_col, s>>>(P->dj, P->Lcol);
         CK(cudaEventRecord(ev[2 * i + 2], s));
     }
     CK(cudaGetLastError());
@@ -728,6 +770,31 @@ int imr_gaussian_blur(float *d_data, float *d_tmp, unsigned W, unsigned H, doubl
         CK(cudaMemcpyAsync(d_data, d_tmp, (size_t)W * H * 4, cudaMemcpyDeviceToDevice, s));
     }
     CK(cudaGetLastError());
+    return IMR_SUCCESS;
+}
+
+int imr_diffraction_intensity(float *h_io, unsigned W, unsigned H, void *stream)
+{
+    if (!h_io || W == 0 || H == 0) return IMR_ERR_INVALID_VALUE;
+    std::vector<int> r;
+    if (!factor_len((int)W, r) || !factor_len((int)H, r)) return IMR_ERR_UNSUPPORTED_SIZE;
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t N = (size_t)W * H;
+    float2 *d = nullptr;
+    float *f = nullptr;
+    CK(cudaMallocAsync((void **)&d, N * 8, s));
+    CK(cudaMallocAsync((void **)&f, N * 4, s));
+    CK(cudaMemcpyAsync(f, h_io, N * 4, cudaMemcpyHostToDevice, s));
+    const int g = (int)std::min<size_t>((N + 255) / 256, 148 * 16);
+    k_real_to_complex<<<g, 256, 0, s>>>(f, d, (long)N);
+    int rc = imr_fft2d(d, W, H, -1, stream);
+    if (rc) return rc;
+    k_complex_norm<<<g, 256, 0, s>>>(d, f, (long)N);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(h_io, f, N * 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaFreeAsync(d, s));
+    CK(cudaFreeAsync(f, s));
+    CK(cudaStreamSynchronize(s));
     return IMR_SUCCESS;
 }
 

@@ -72,10 +72,16 @@ struct alignas(64) JobDev {
     int n_row_tiles, n_col_tiles, n_vb_tiles, vb_tiles_x;
 };
 
-// One CTA's assignment: job index and tile index within that job.
+// One unit of work: job index and tile (row group / column group) index.
 struct WorkItem {
     int job;
     int tile;
+};
+
+// A launch's items, in device memory.  items == nullptr: job 0, tiles 0..n-1.
+struct WorkList {
+    const WorkItem *items;
+    int n;
 };
 
 }  // namespace imr

@@ -20,29 +20,29 @@ int build_weight_table(const imr_params &p, std::vector<float> &w, std::vector<i
 
 // Kernels and launch shape of the row passes for one row length.
 struct RowKernels {
-    void (*hio_first)(const JobDev *, const WorkItem *);
-    void (*hio)(const JobDev *, const WorkItem *);
-    void (*finish)(const JobDev *, const WorkItem *, float2 *);
+    void (*hio_first)(const JobDev *, const WorkList *);
+    void (*hio)(const JobDev *, const WorkList *);
+    void (*finish)(const JobDev *, const WorkList *, float2 *);
     void (*fft_fwd)(float2 *, FftPlanDev, int, int);
     void (*fft_inv)(float2 *, FftPlanDev, int, int);
     int nb;        // rows per CTA
     int threads;
     int smem;      // dynamic shared memory of the FFT kernels (bytes); 0: nb*N*8
     // pipelined (persistent, TMA) row passes; null when the length has none
-    void (*p_hio_first)(const JobDev *, const WorkItem *, int);
-    void (*p_hio)(const JobDev *, const WorkItem *, int);
+    void (*p_hio_first)(const JobDev *, const WorkList *);
+    void (*p_hio)(const JobDev *, const WorkList *);
     int p_smem_first, p_smem;
 };
 // Kernels and launch shape of the column passes for one column length.
 struct ColKernels {
-    void (*col)(const JobDev *, const WorkItem *);
-    void (*init)(const JobDev *, const WorkItem *);
+    void (*col)(const JobDev *, const WorkList *);
+    void (*init)(const JobDev *, const WorkList *);
     void (*fft_fwd)(float2 *, FftPlanDev, int, int);
     void (*fft_inv)(float2 *, FftPlanDev, int, int);
     int nb;        // columns per CTA
     int threads;
     int smem;      // dynamic shared memory (bytes); 0: nb*N*8
-    void (*p_col)(const JobDev *, const WorkItem *, int);   // pipelined column pass or null
+    void (*p_col)(const JobDev *, const WorkList *);   // pipelined column pass or null
     int p_smem;
     int p_box_rows;  // rows per 2D TMA box
     int p_tma_m;     // 1: the modulus tile also arrives by TMA
@@ -54,6 +54,21 @@ int persistent_grid(const void *kernel, int threads, int smem, int items);
 // 2D tensor map over a row-major [H][W] array of `elem`-byte elements with a
 // (box_w, box_h) box; returns false when the shape cannot be described.
 bool encode_tensor_map(CUtensorMap *map, const void *base, int W, int H, int elem, int box_w, int box_h);
+
+// Host description of one reconstruction's device layout and kernels.
+struct JobShape {
+    RowKernels rk{};
+    ColKernels ck{};
+    bool p_rows = false, p_cols = false;
+    size_t smem_row = 0, smem_fin = 0, smem_col = 0;
+    size_t bytes = 0;   // arena bytes (JobState not included)
+    size_t oX = 0, oG = 0, oM = 0, oHB = 0, oVB = 0, oOut = 0, oMask = 0, oW = 0, oT = 0, oEP = 0, oErr = 0;
+    std::vector<float> wt;
+    std::vector<int> taps;
+};
+int job_prepare(unsigned W, unsigned H, const imr_params &p, JobDev &J, JobShape &S);
+void job_bind(JobDev &J, JobShape &S, char *arena, JobState *st);
+int job_upload(const JobDev &J, const JobShape &S, char *arena, JobDev *dj, cudaStream_t s);
 int plan_cache_acquire(unsigned W, unsigned H, const imr_params *params, imr_plan **out);
 void plan_cache_release(imr_plan *P);
 

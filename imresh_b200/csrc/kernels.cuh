@@ -26,18 +26,26 @@
 
 namespace imr {
 
-__device__ __forceinline__ WorkItem get_work(const WorkItem *wl)
+
+// Item i of a work list (a null item array means job 0, tile i).
+__device__ __forceinline__ WorkItem item_at(const WorkList *L, int i)
 {
-    if (wl) return wl[blockIdx.x];
-    return WorkItem{0, (int)blockIdx.x};
+    if (L->items) return L->items[i];
+    return WorkItem{0, i};
 }
 
-// work item `item` of a persistent launch (a null list means job 0, tile item)
-__device__ __forceinline__ WorkItem get_work_at(const WorkItem *wl, int item)
-{
-    if (wl) return wl[item];
-    return WorkItem{0, item};
-}
+// Kernel wrapper: the CTAs stride over the list's items, so one launch with a
+// fixed grid serves any number of items (the count lives in device memory and
+// may change between replays of a captured graph).
+#define IMR_ITEM_LOOP(BODY_CALL)                                        \
+    do {                                                                \
+        const int n_items_ = L->n;                                      \
+        for (int it_ = blockIdx.x; it_ < n_items_; it_ += gridDim.x) {  \
+            const WorkItem wi = item_at(L, it_);                        \
+            BODY_CALL;                                                  \
+            __syncthreads();                                            \
+        }                                                               \
+    } while (0)
 
 // ---- launch shapes ---------------------------------------------------------
 // Row passes: NB rows of length N per CTA, T threads.  Column passes: NB
@@ -166,11 +174,10 @@ __device__ __forceinline__ float vblur_tile(const float *src, float *dst, int W,
 // X := inverse column FFT of (M, 0): the column half of g'_0 = IFFT2(M)
 // (cudaShrinkWrap.cu:229-232: CopyToRealPart then an in-place inverse FFT).
 template <int N>
-__global__ void __launch_bounds__(col_threads(N)) k_col_init(const JobDev *jobs, const WorkItem *wl)
+__device__ __forceinline__ void b_col_init(const JobDev *jobs, const WorkItem wi)
 {
     extern __shared__ float4 smem4[];
     float2 *sm = reinterpret_cast<float2 *>(smem4);
-    const WorkItem wi = get_work(wl);
     const JobDev &J = jobs[wi.job];
     const int W = J.W, H = J.H;
     const int x0 = wi.tile * J.cpc;
@@ -188,17 +195,21 @@ __global__ void __launch_bounds__(col_threads(N)) k_col_init(const JobDev *jobs,
         J.X[(size_t)y * W + x0 + c] = sm[y * es + c];
     }
 }
+template <int N>
+__global__ void __launch_bounds__(col_threads(N)) k_col_init(const JobDev *jobs, const WorkList *L)
+{
+    IMR_ITEM_LOOP((b_col_init<N>(jobs, wi)));
+}
 
 // ---------------------------------------------------------------- column pass
 // Forward column FFT, G <- G * M/|G| (|G| = 0 -> 1; applyComplexModulus,
 // src/imresh/algorithms/cuda/cudaVectorElementwise.cu:168-195), inverse
 // column FFT.
 template <int N>
-__global__ void __launch_bounds__(col_threads(N)) k_col(const JobDev *jobs, const WorkItem *wl)
+__device__ __forceinline__ void b_col(const JobDev *jobs, const WorkItem wi)
 {
     extern __shared__ float4 smem4[];
     float2 *sm = reinterpret_cast<float2 *>(smem4);
-    const WorkItem wi = get_work(wl);
     const JobDev &J = jobs[wi.job];
     if (J.st->stop) return;
     const int W = J.W, H = J.H;
@@ -227,6 +238,11 @@ __global__ void __launch_bounds__(col_threads(N)) k_col(const JobDev *jobs, cons
         J.X[(size_t)y * W + x0 + c] = sm[y * es + c];
     }
 }
+template <int N>
+__global__ void __launch_bounds__(col_threads(N)) k_col(const JobDev *jobs, const WorkList *L)
+{
+    IMR_ITEM_LOOP((b_col<N>(jobs, wi)));
+}
 
 // ---------------------------------------------------------------- row pass
 // Inverse row FFT -> g'; HIO domain constraint
@@ -237,11 +253,10 @@ __global__ void __launch_bounds__(col_threads(N)) k_col(const JobDev *jobs, cons
 // image (mask = blurred < threshold, cudaKernelCutOff, cudaVectorElementwise.cu:198-219)
 // and, on cycle 0, takes g_prev = g'_0 (cudaShrinkWrap.cu:304-309).
 template <bool FIRST, int N>
-__global__ void __launch_bounds__(row_threads(N)) k_row_hio(const JobDev *jobs, const WorkItem *wl)
+__device__ __forceinline__ void b_row_hio(const JobDev *jobs, const WorkItem wi)
 {
     extern __shared__ float4 smem4[];
     float2 *sm = reinterpret_cast<float2 *>(smem4);
-    const WorkItem wi = get_work(wl);
     const JobDev &J = jobs[wi.job];
     JobState *st = J.st;
     if (st->stop) return;
@@ -281,21 +296,24 @@ __global__ void __launch_bounds__(row_threads(N)) k_row_hio(const JobDev *jobs, 
     fft_rows<N, -1>(sm, nr, J.prow);
     for (int i = threadIdx.x; i < n; i += T) J.X[base + i] = sm[i];
 }
+template <bool FIRST, int N>
+__global__ void __launch_bounds__(row_threads(N)) k_row_hio(const JobDev *jobs, const WorkList *L)
+{
+    IMR_ITEM_LOOP((b_row_hio<FIRST, N>(jobs, wi)));
+}
 
 // Once per cycle: inverse row FFT -> g'; out = Re(g') (CopyFromRealPart,
 // cudaVectorElementwise.cu:98-117); error sums against the previous cycle's
 // mask (cudaKernelCalculateHioError, cudaVectorReduce.cu:284-355, summed in
 // double here); |g'| (cudaKernelComplexNormElementwise) blurred along rows.
 template <int N>
-__global__ void __launch_bounds__(row_threads(N)) k_row_finish(const JobDev *jobs, const WorkItem *wl,
-                                                              float2 *dbg_gprime)
+__device__ __forceinline__ void b_row_finish(const JobDev *jobs, const WorkItem wi, float2 *dbg_gprime)
 {
     extern __shared__ float4 smem4[];
     float2 *sm = reinterpret_cast<float2 *>(smem4);
     constexpr int T = row_threads(N);
     __shared__ float wsm[kTapStride];
     __shared__ double red[2 * T / 32];
-    const WorkItem wi = get_work(wl);
     const JobDev &J = jobs[wi.job];
     JobState *st = J.st;
     if (st->stop) return;
@@ -335,20 +353,24 @@ __global__ void __launch_bounds__(row_threads(N)) k_row_finish(const JobDev *job
         J.hb[base + i] = hblur_at(nrm + r * W, W, x, wsm, K);
     }
 }
+template <int N>
+__global__ void __launch_bounds__(row_threads(N)) k_row_finish(const JobDev *jobs, const WorkList *L, float2 *dbg_gprime)
+{
+    IMR_ITEM_LOOP((b_row_finish<N>(jobs, wi, dbg_gprime)));
+}
 
 // Once per cycle: vertical blur hb -> vb and the global max; the last CTA
 // of the job finalises the cycle: error E = sqrt(sum mask*|g'|)/sum mask of
 // the previous cycle (cudaVectorReduce.cu:357-403) and the stop test
 // E < target (cudaShrinkWrap.cu:374-375), then the threshold
 // (cycle 0 ? cutOffAutoCorel : cutOff) * max (cudaShrinkWrap.cu:274-276).
-__global__ void __launch_bounds__(kVbThreads) k_vblur(const JobDev *jobs, const WorkItem *wl)
+__device__ __forceinline__ void b_vblur(const JobDev *jobs, const WorkItem wi)
 {
     __shared__ float tile[(kVbTileY + 2 * 31) * kVbTileX];
     __shared__ float wsm[kTapStride];
     __shared__ float fred[kVbThreads / 32];
     __shared__ double red[2 * kVbThreads / 32];
     __shared__ int s_last;
-    const WorkItem wi = get_work(wl);
     const JobDev &J = jobs[wi.job];
     JobState *st = J.st;
     if (st->stop) return;
@@ -393,6 +415,10 @@ __global__ void __launch_bounds__(kVbThreads) k_vblur(const JobDev *jobs, const 
         if (stop) st->stop = 1;
         __threadfence();
     }
+}
+static __global__ void __launch_bounds__(kVbThreads) k_vblur(const JobDev *jobs, const WorkList *L)
+{
+    IMR_ITEM_LOOP((b_vblur(jobs, wi)));
 }
 
 // ---------------------------------------------------------------- plain FFT
@@ -441,7 +467,7 @@ struct Taps {
     float w[kTapStride];
 };
 
-__global__ void __launch_bounds__(kRowThreads) k_hblur(float *data, int W, int H, Taps w, int K)
+static __global__ void __launch_bounds__(kRowThreads) k_hblur(float *data, int W, int H, Taps w, int K)
 {
     extern __shared__ float4 smem4[];
     float *row = reinterpret_cast<float *>(smem4);
@@ -453,7 +479,7 @@ __global__ void __launch_bounds__(kRowThreads) k_hblur(float *data, int W, int H
     for (int x = threadIdx.x; x < W; x += kRowThreads) data[base + x] = hblur_at(row, W, x, wsm, K);
 }
 
-__global__ void __launch_bounds__(kVbThreads) k_vblur_plain(const float *src, float *dst, int W, int H,
+static __global__ void __launch_bounds__(kVbThreads) k_vblur_plain(const float *src, float *dst, int W, int H,
                                                            Taps w, int K, unsigned *max_bits)
 {
     __shared__ float tile[(kVbTileY + 2 * 31) * kVbTileX];
@@ -468,6 +494,18 @@ __global__ void __launch_bounds__(kVbThreads) k_vblur_plain(const float *src, fl
     if (threadIdx.x == 0 && max_bits) atomicMax(max_bits, __float_as_uint(mx));
 }
 
+// (x, 0) <-> |z| helpers of the forward model
+static __global__ void k_real_to_complex(const float *src, float2 *dst, long n)
+{
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        dst[i] = make_float2(src[i], 0.f);
+}
+static __global__ void k_complex_norm(const float2 *src, float *dst, long n)
+{
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        dst[i] = cnorm_ref(src[i]);
+}
+
 // Global max of a float array (vectorMax; cudaVectorReduce.cu:229-239):
 // signed floats ordered through an order-preserving integer key.
 __device__ __forceinline__ unsigned f2key(float f)
@@ -475,7 +513,7 @@ __device__ __forceinline__ unsigned f2key(float f)
     unsigned u = __float_as_uint(f);
     return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
 }
-__global__ void __launch_bounds__(256) k_vector_max(const float *d, long n, unsigned *key)
+static __global__ void __launch_bounds__(256) k_vector_max(const float *d, long n, unsigned *key)
 {
     __shared__ unsigned s[8];
     unsigned m = 0u;   // key of the lowest value
@@ -509,12 +547,11 @@ __host__ __device__ constexpr int rcol_smem(int N) { return reg_smem_bytes(N, rc
 
 // X := inverse column FFT of (M, 0)
 template <int N>
-__global__ void __launch_bounds__(rcol_threads(N)) k_col_init_r(const JobDev *jobs, const WorkItem *wl)
+__device__ __forceinline__ void b_col_init_r(const JobDev *jobs, const WorkItem wi)
 {
     extern __shared__ float4 smem4[];
     float2 *sm = reinterpret_cast<float2 *>(smem4);
     constexpr int NB = rcol_nb(N), Q = N / 8;
-    const WorkItem wi = get_work(wl);
     const JobDev &J = jobs[wi.job];
     const int W = J.W;
     const int b = threadIdx.x % NB, l = threadIdx.x / NB;
@@ -530,15 +567,19 @@ __global__ void __launch_bounds__(rcol_threads(N)) k_col_init_r(const JobDev *jo
         for (int m = 0; m < 8; ++m) J.X[(size_t)(l + m * Q) * W + x] = v[m];
     }
 }
+template <int N>
+__global__ void __launch_bounds__(rcol_threads(N)) k_col_init_r(const JobDev *jobs, const WorkList *L)
+{
+    IMR_ITEM_LOOP((b_col_init_r<N>(jobs, wi)));
+}
 
 // column pass: forward column FFT, modulus projection, inverse column FFT
 template <int N>
-__global__ void __launch_bounds__(rcol_threads(N)) k_col_r(const JobDev *jobs, const WorkItem *wl)
+__device__ __forceinline__ void b_col_r(const JobDev *jobs, const WorkItem wi)
 {
     extern __shared__ float4 smem4[];
     float2 *sm = reinterpret_cast<float2 *>(smem4);
     constexpr int NB = rcol_nb(N), Q = N / 8;
-    const WorkItem wi = get_work(wl);
     const JobDev &J = jobs[wi.job];
     if (J.st->stop) return;
     const int W = J.W;
@@ -563,15 +604,19 @@ __global__ void __launch_bounds__(rcol_threads(N)) k_col_r(const JobDev *jobs, c
         for (int m = 0; m < 8; ++m) J.X[(size_t)(l + m * Q) * W + x] = v[m];
     }
 }
+template <int N>
+__global__ void __launch_bounds__(rcol_threads(N)) k_col_r(const JobDev *jobs, const WorkList *L)
+{
+    IMR_ITEM_LOOP((b_col_r<N>(jobs, wi)));
+}
 
 // row pass: inverse row FFT, HIO update, forward row FFT (see k_row_hio)
 template <bool FIRST, int N>
-__global__ void __launch_bounds__(rrow_threads(N)) k_row_hio_r(const JobDev *jobs, const WorkItem *wl)
+__device__ __forceinline__ void b_row_hio_r(const JobDev *jobs, const WorkItem wi)
 {
     extern __shared__ float4 smem4[];
     float2 *sm = reinterpret_cast<float2 *>(smem4);
     constexpr int Q = N / 8;
-    const WorkItem wi = get_work(wl);
     const JobDev &J = jobs[wi.job];
     JobState *st = J.st;
     if (st->stop) return;
@@ -615,18 +660,21 @@ __global__ void __launch_bounds__(rrow_threads(N)) k_row_hio_r(const JobDev *job
         for (int m = 0; m < 8; ++m) J.X[base + l + m * Q] = v[m];
     }
 }
+template <bool FIRST, int N>
+__global__ void __launch_bounds__(rrow_threads(N)) k_row_hio_r(const JobDev *jobs, const WorkList *L)
+{
+    IMR_ITEM_LOOP((b_row_hio_r<FIRST, N>(jobs, wi)));
+}
 
 // once per cycle: inverse row FFT -> g'; out, error sums, |g'| blurred along rows
 template <int N>
-__global__ void __launch_bounds__(rrow_threads(N)) k_row_finish_r(const JobDev *jobs, const WorkItem *wl,
-                                                                 float2 *dbg_gprime)
+__device__ __forceinline__ void b_row_finish_r(const JobDev *jobs, const WorkItem wi, float2 *dbg_gprime)
 {
     extern __shared__ float4 smem4[];
     float2 *sm = reinterpret_cast<float2 *>(smem4);
     constexpr int T = rrow_threads(N), Q = N / 8;
     __shared__ float wsm[kTapStride];
     __shared__ double red[2 * T / 32 > 2 ? 2 * T / 32 : 2];
-    const WorkItem wi = get_work(wl);
     const JobDev &J = jobs[wi.job];
     JobState *st = J.st;
     if (st->stop) return;
@@ -671,6 +719,11 @@ __global__ void __launch_bounds__(rrow_threads(N)) k_row_finish_r(const JobDev *
             J.hb[base + e] = hblur_at(nrow, N, e, wsm, K);
         }
     }
+}
+template <int N>
+__global__ void __launch_bounds__(rrow_threads(N)) k_row_finish_r(const JobDev *jobs, const WorkList *L, float2 *dbg_gprime)
+{
+    IMR_ITEM_LOOP((b_row_finish_r<N>(jobs, wi, dbg_gprime)));
 }
 
 // plain 2D transform passes
@@ -740,15 +793,14 @@ __host__ __device__ constexpr int prow_stage_bytes()
 template <bool FIRST, int N>
 __host__ __device__ constexpr int prow_smem() { return 128 + 2 * prow_stage_bytes<FIRST, N>(); }
 
-__device__ __forceinline__ bool job_live(const JobDev *jobs, const WorkItem *wl, int item)
+__device__ __forceinline__ bool job_live(const JobDev *jobs, const WorkList *L, int item)
 {
-    const WorkItem wi = get_work_at(wl, item);
+    const WorkItem wi = item_at(L, item);
     return jobs[wi.job].st->stop == 0;
 }
 
 template <bool FIRST, int N>
-__global__ void __launch_bounds__(rrow_threads(N)) k_row_hio_p(const JobDev *jobs, const WorkItem *wl,
-                                                              int n_items)
+__global__ void __launch_bounds__(rrow_threads(N)) k_row_hio_p(const JobDev *jobs, const WorkList *L)
 {
     extern __shared__ __align__(128) unsigned char sbuf[];
     constexpr int NB = rrow_nb(N), Q = N / 8;
@@ -757,13 +809,14 @@ __global__ void __launch_bounds__(rrow_threads(N)) k_row_hio_p(const JobDev *job
     uint64_t *bars = reinterpret_cast<uint64_t *>(sbuf);
     unsigned char *stages = sbuf + 128;
     const int b = threadIdx.x / Q, l = threadIdx.x % Q;
+    const int n_items = L->n;
 
     auto next_live = [&](int it) {
-        while (it < n_items && !job_live(jobs, wl, it)) it += gridDim.x;
+        while (it < n_items && !job_live(jobs, L, it)) it += gridDim.x;
         return it;
     };
     auto issue = [&](int item, int s) {   // one thread
-        const WorkItem wi = get_work_at(wl, item);
+        const WorkItem wi = item_at(L, item);
         const JobDev &J = jobs[wi.job];
         const int y0 = wi.tile * J.rpc;
         const int nr = min(J.rpc, J.H - y0);
@@ -792,7 +845,7 @@ __global__ void __launch_bounds__(rrow_threads(N)) k_row_hio_p(const JobDev *job
             fence_proxy_async_smem();
             issue(nxt, s ^ 1);
         }
-        const WorkItem wi = get_work_at(wl, item);
+        const WorkItem wi = item_at(L, item);
         const JobDev &J = jobs[wi.job];
         JobState *st = J.st;
         const bool landed = mbar_wait(&bars[s], (uint32_t)((k >> 1) & 1));
@@ -860,7 +913,7 @@ template <int N>
 __host__ __device__ constexpr int pcol_smem() { return 128 + 2 * pcol_stage_bytes<N>(); }
 
 template <int N>
-__global__ void __launch_bounds__(rcol_threads(N)) k_col_p(const JobDev *jobs, const WorkItem *wl, int n_items)
+__global__ void __launch_bounds__(rcol_threads(N)) k_col_p(const JobDev *jobs, const WorkList *L)
 {
     extern __shared__ __align__(128) unsigned char sbuf[];
     constexpr int NB = rcol_nb(N), Q = N / 8;
@@ -871,13 +924,14 @@ __global__ void __launch_bounds__(rcol_threads(N)) k_col_p(const JobDev *jobs, c
     uint64_t *bars = reinterpret_cast<uint64_t *>(sbuf);
     unsigned char *stages = sbuf + 128;
     const int b = threadIdx.x % NB, l = threadIdx.x / NB;
+    const int n_items = L->n;
 
     auto next_live = [&](int it) {
-        while (it < n_items && !job_live(jobs, wl, it)) it += gridDim.x;
+        while (it < n_items && !job_live(jobs, L, it)) it += gridDim.x;
         return it;
     };
     auto issue = [&](int item, int s) {
-        const WorkItem wi = get_work_at(wl, item);
+        const WorkItem wi = item_at(L, item);
         const JobDev &J = jobs[wi.job];
         const int x0 = wi.tile * NB;
         unsigned char *st = stages + s * STAGE;
@@ -903,7 +957,7 @@ __global__ void __launch_bounds__(rcol_threads(N)) k_col_p(const JobDev *jobs, c
             fence_proxy_async_smem();
             issue(nxt, s ^ 1);
         }
-        const WorkItem wi = get_work_at(wl, item);
+        const WorkItem wi = item_at(L, item);
         const JobDev &J = jobs[wi.job];
         const bool landed = mbar_wait(&bars[s], (uint32_t)((k >> 1) & 1));
         if (__syncthreads_or(!landed)) {

@@ -129,9 +129,58 @@ int imr_gaussian_blur(float *d_data, float *d_tmp, unsigned W, unsigned H, doubl
  * src/imresh/libs/calcGaussianKernel.cpp:42-91); returns the tap count, and
  * writes the weights when it is <= cap. */
 int imr_gaussian_weights(double sigma, float *h_weights, int cap);
+/* Forward model |FFT2(object)| (the Fourier modulus) of a real W*H image,
+ * in place in HOST memory, on the engine's FFT; synchronous
+ * (diffractionIntensity, src/imresh/libs/diffractionIntensity.cpp:84-135). */
+int imr_diffraction_intensity(float *h_io, unsigned W, unsigned H, void *stream);
 /* Global maximum of n floats (cudaVectorMax, cudaVectorReduce.cu:229-239);
  * the result goes to HOST *h_max; synchronous. */
 int imr_vector_max(const float *d_data, size_t n, float *h_max, void *stream);
+
+/* ------------------------------------------------------------------------
+ * Batched, continuously-admitting engine (the served form of the path).
+ * Replaces the reference's per-task std::thread + stream round robin
+ * (imresh::io::taskQueue*, src/imresh/io/taskQueue.cu:91-251) with device-
+ * resident state for every admitted reconstruction: one imr_engine_step runs
+ * one shrink-wrap cycle of every active reconstruction, whatever their sizes,
+ * admits pending requests while the device-memory budget allows, and retires
+ * finished ones (their Re(g') is copied to the caller's h_out).  Not thread
+ * safe: drive one engine from one thread.
+ */
+typedef struct imr_engine imr_engine;
+
+typedef struct imr_result {
+    long long tag;         /* the caller's tag from imr_engine_submit        */
+    unsigned width, height;
+    int cycles_done;       /* HIO blocks run and error-tested                */
+    float last_error;      /* error after the last of them                   */
+    double latency_ms;     /* submit -> result in h_out                      */
+    int status;            /* imr_status of this reconstruction              */
+} imr_result;
+
+typedef struct imr_engine_info {
+    int pending, active, done;
+    size_t device_bytes_used, device_bytes_peak, device_bytes_budget;
+    long launches;         /* kernel launches issued so far                  */
+    long steps;
+} imr_engine_info;
+
+/* device_bytes: admission budget (0 = 80 % of the free device memory);
+ * max_jobs: reconstructions resident at once. */
+int imr_engine_create(imr_engine **engine, size_t device_bytes, int max_jobs, void *stream);
+/* Queue one reconstruction.  h_modulus (W*H floats) must stay valid until the
+ * request is admitted, h_out (W*H floats) until its result is polled. */
+int imr_engine_submit(imr_engine *engine, const float *h_modulus, float *h_out, unsigned W,
+                      unsigned H, const imr_params *params, long long tag);
+/* Admit, run one cycle of every active reconstruction, retire finished ones.
+ * Synchronous. */
+int imr_engine_step(imr_engine *engine);
+/* Step until nothing is pending or active. */
+int imr_engine_run(imr_engine *engine);
+/* Finished reconstructions since the last poll (up to max_results). */
+int imr_engine_poll(imr_engine *engine, imr_result *results, int max_results, int *n_results);
+int imr_engine_stats(imr_engine *engine, imr_engine_info *info);
+int imr_engine_destroy(imr_engine *engine);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,80 @@
+// A caller written against the reference's own API, the way its examples use
+// it (examples/miniExample.cpp:102-116, examples/threadedExample.cpp:44-113):
+// build an object, turn it into a Fourier modulus with diffractionIntensity,
+// reconstruct it with cudaShrinkWrap, then run a batch through the task
+// queue.  Compiled against include/imresh (the reference's header paths) and
+// linked against libimresh_b200.so only.  Prints "OK" on success.
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "algorithms/cuda/cudaShrinkWrap.hpp"
+#include "io/taskQueue.cu"
+#include "io/writeOutFuncs/writeOutFuncs.hpp"
+#include "libs/diffractionIntensity.hpp"
+
+// a few Gaussian blobs near the centre (deterministic)
+static float *make_object(unsigned W, unsigned H)
+{
+    float *p = new float[W * H];
+    std::memset(p, 0, sizeof(float) * W * H);
+    const float cx[5] = {0.50f, 0.45f, 0.56f, 0.52f, 0.47f}, cy[5] = {0.50f, 0.54f, 0.47f, 0.58f, 0.44f};
+    for (int b = 0; b < 5; ++b)
+        for (unsigned y = 0; y < H; ++y)
+            for (unsigned x = 0; x < W; ++x) {
+                const float dx = x - cx[b] * W, dy = y - cy[b] * H;
+                p[y * W + x] += std::exp(-(dx * dx + dy * dy) / 8.f);
+            }
+    return p;
+}
+
+static bool finite(const float *p, size_t n)
+{
+    for (size_t i = 0; i < n; ++i)
+        if (!std::isfinite(p[i])) return false;
+    return true;
+}
+
+int main()
+{
+    const unsigned W = 256, H = 192;
+    float *pData = make_object(W, H);
+    imresh::libs::diffractionIntensity(pData, W, H);
+    std::vector<float> modulus(pData, pData + W * H);
+
+    // miniExample's call: 96 blocks x 256 threads (ignored), 64 cycles,
+    // target 1e-6, default beta, autocorrelation cutoff 0.001, cutoff 0.01
+    int rc = imresh::algorithms::cuda::cudaShrinkWrap(pData, W, H, cudaStream_t(0), 96, 256, 64, 1e-6, 0,
+                                                        0.001, 0.01, 0, 0);
+    if (rc != 0 || !finite(pData, W * H)) {
+        std::printf("cudaShrinkWrap failed: rc=%d\n", rc);
+        return 1;
+    }
+    delete[] pData;
+
+    // threadedExample's pattern: init, N tasks with a write-out callback, deinit
+    imresh::io::taskQueueInit();
+    std::atomic<int> finished{0}, bad{0};
+    const int nTasks = 12;
+    for (int i = 0; i < nTasks; ++i) {
+        float *task = new float[W * H];
+        std::memcpy(task, modulus.data(), sizeof(float) * W * H);
+        imresh::io::addTask(task, W, H,
+                            [&](float *mem, unsigned const w, unsigned const h, std::string name) {
+                                if (w != W || h != H || !finite(mem, (size_t)w * h) || name.empty()) ++bad;
+                                ++finished;
+                                imresh::io::writeOutFuncs::justFree(mem, w, h, name);
+                            },
+                            "task_" + std::to_string(i), 4 + i % 3 /* cycles */);
+    }
+    imresh::io::taskQueueDeinit();
+    if (finished != nTasks || bad != 0) {
+        std::printf("task queue: finished %d of %d, bad %d\n", (int)finished, nTasks, (int)bad);
+        return 1;
+    }
+    std::printf("OK\n");
+    return 0;
+}

@@ -3,6 +3,7 @@ GPU, exports every function include/imresh_b200.h declares, and its host-side
 logic (status strings, supported lengths, Gaussian weights, parameter
 validation that needs no device) behaves as documented."""
 import ctypes as C
+import os
 
 import numpy as np
 import pytest
@@ -50,3 +51,20 @@ def test_invalid_arguments_rejected_without_device():
     h = C.c_void_p()
     assert L.imr_plan_create(C.byref(h), 0, 4, None) == 1
     assert L.imr_plan_destroy(None) == 0
+
+
+def test_cpp_drop_in_compiles_and_links(tmp_path):
+    """A caller written against the reference's C++ API (header paths,
+    namespaces, default arguments) builds and links against the library."""
+    from tests.cpp_build import build_drop_in
+    exe = build_drop_in(str(tmp_path))
+    assert os.path.exists(exe)
+
+
+def test_reference_symbols_exported():
+    import subprocess
+    out = subprocess.run(["nm", "-DC", imr.LIB_PATH], capture_output=True, text=True).stdout
+    for sym in ("imresh::algorithms::cuda::cudaShrinkWrap(", "imresh::io::taskQueueInit()",
+                "imresh::io::taskQueueDeinit()", "imresh::io::addTask(",
+                "imresh::io::writeOutFuncs::justFree(", "imresh::libs::diffractionIntensity("):
+        assert sym in out, sym
