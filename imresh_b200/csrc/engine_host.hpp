@@ -10,6 +10,7 @@ namespace imr {
 constexpr unsigned kMaxSide = 4096;
 constexpr int kMaxRuntimeSide = 2048;
 
+extern thread_local char g_last_error[256];   // imr_last_error() text
 void set_error(const char *what, cudaError_t e);
 bool factor_len(int n, std::vector<int> &rad);
 int make_fft_plan(int n, FftPlanDev &p);

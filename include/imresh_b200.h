@@ -138,6 +138,23 @@ int imr_diffraction_intensity(float *h_io, unsigned W, unsigned H, void *stream)
 int imr_vector_max(const float *d_data, size_t n, float *h_max, void *stream);
 
 /* ------------------------------------------------------------------------
+ * Reconstruction that allocates nothing -- no counterpart in the reference.
+ * For callers that cannot call cudaMalloc (memory owned by a fixed arena or a
+ * framework allocator, loops that must not take the driver's allocation
+ * locks, processes that reserve all device memory up front).  d_modulus and
+ * d_out are DEVICE buffers of W*H floats owned by the caller; all other
+ * working memory is a static device array of the library, so W*H is limited
+ * to 512*512 pixels (IMR_ERR_UNSUPPORTED_SIZE beyond, with a message in
+ * imr_last_error) and nCycles to 1024.  Asynchronous on `stream`.  The first
+ * call on a device looks up the array's address and sets kernel attributes:
+ * make it before any stream capture.  All calls share the one array: calls
+ * whose GPU work overlaps (different streams, unordered host threads) race;
+ * issue them one after another on one stream.
+ */
+int imr_shrink_wrap_noalloc(const float *d_modulus, float *d_out, unsigned W, unsigned H,
+                            const imr_params *params, void *stream);
+
+/* ------------------------------------------------------------------------
  * Batched, continuously-admitting engine (the served form of the path).
  * Replaces the reference's per-task std::thread + stream round robin
  * (imresh::io::taskQueue*, src/imresh/io/taskQueue.cu:91-251) with device-
