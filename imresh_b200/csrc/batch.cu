@@ -265,8 +265,8 @@ static int launch_step(imr_engine *E, const std::vector<EJob *> &fresh)
             const WorkList *Li = L + g.list_base + 1 + i;
             const int n = g.hio_count[i];
             if (g.pipelined)
-                g.ck.p_col<<<persistent_grid((const void *)g.ck.p_col, g.ck.threads, g.ck.p_smem, n), g.ck.threads,
-                             g.ck.p_smem, s>>>(E->dj, Li);
+                g.ck.p_col<<<persistent_grid((const void *)g.ck.p_col, g.ck.p_threads, g.ck.p_smem, n),
+                             g.ck.p_threads, g.ck.p_smem, s>>>(E->dj, Li);
             else
                 g.ck.col<<<loop_grid(E, n), g.ck.threads, g.smem, s>>>(E->dj, Li);
             ++E->launches;

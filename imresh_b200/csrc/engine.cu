@@ -130,13 +130,13 @@ static ColKernels col_set()
     if constexpr (N >= 16 && is_pow2(N))
         return ColKernels{k_col_r<N>, k_col_init_r<N>, k_fft_cols_r<-1, N>, k_fft_cols_r<+1, N>,
                           rcol_nb(N), rcol_threads(N), rcol_smem(N), k_col_p<N>, pcol_smem<N>(),
-                          pcol_box_rows(N), pcol_tma_m(N) ? 1 : 0};
+                          pcol_box_rows(N), pcol_tma_m(N) ? 1 : 0, pcol_threads(N)};
     else if constexpr (N >= 8 && is_pow2(N))
         return ColKernels{k_col_r<N>, k_col_init_r<N>, k_fft_cols_r<-1, N>, k_fft_cols_r<+1, N>,
-                          rcol_nb(N), rcol_threads(N), rcol_smem(N), nullptr, 0, 0, 0};
+                          rcol_nb(N), rcol_threads(N), rcol_smem(N), nullptr, 0, 0, 0, 0};
     else
         return ColKernels{k_col<N>, k_col_init<N>, k_fft_cols<-1, N>, k_fft_cols<+1, N>, col_nb(N),
-                          col_threads(N), 0, nullptr, 0, 0, 0};
+                          col_threads(N), 0, nullptr, 0, 0, 0, 0};
 }
 
 int persistent_grid(const void *kernel, int threads, int smem, int items)
@@ -336,7 +336,7 @@ static int plan_launch_cycle(imr_plan *P, cudaStream_t s)
             (i == 0 ? rk.hio_first : rk.hio)<<<J.n_row_tiles, rk.threads, P->smem_row, s>>>(P->dj, P->Lrow);
         }
         if (P->p_cols)
-            ck.p_col<<<P->g_col, ck.threads, ck.p_smem, s>>>(P->dj, P->Lcol);
+            ck.p_col<<<P->g_col, ck.p_threads, ck.p_smem, s>>>(P->dj, P->Lcol);
         else
             ck.col<<<J.n_col_tiles, ck.threads, P->smem_col, s>>>(P->dj, P->Lcol);
     }
@@ -548,7 +548,7 @@ int imr_plan_create(imr_plan **out, unsigned W, unsigned H, const imr_params *pa
         P->g_row = persistent_grid((const void *)P->rk.p_hio, P->rk.threads, P->rk.p_smem, J.n_row_tiles);
     }
     if (P->p_cols)
-        P->g_col = persistent_grid((const void *)P->ck.p_col, P->ck.threads, P->ck.p_smem, J.n_col_tiles);
+        P->g_col = persistent_grid((const void *)P->ck.p_col, P->ck.p_threads, P->ck.p_smem, J.n_col_tiles);
     const WorkList lists[3] = {{nullptr, J.n_row_tiles}, {nullptr, J.n_col_tiles}, {nullptr, J.n_vb_tiles}};
     e = cudaMemcpy(P->Lrow, lists, sizeof(lists), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = job_upload(J, S, a, P->dj, 0) ? cudaErrorUnknown : cudaSuccess;
@@ -675,7 +675,7 @@ int imr_plan_profile(imr_plan *P, int iters, void *stream, float *ms_row, float 
             P->rk.hio<<<J.n_row_tiles, P->rk.threads, P->smem_row, s>>>(P->dj, P->Lrow);
         CK(cudaEventRecord(ev[2 * i + 1], s));
         if (P->p_cols)
-            P->ck.p_col<<<P->g_col, P->ck.threads, P->ck.p_smem, s>>>(P->dj, P->Lcol);
+            P->ck.p_col<<<P->g_col, P->ck.p_threads, P->ck.p_smem, s>>>(P->dj, P->Lcol);
         else
             P->ck.col<<<J.n_col_tiles, P->ck.threads, P->smem_col, s>>>(P->dj, P->Lcol);
         CK(cudaEventRecord(ev[2 * i + 2], s));

@@ -47,6 +47,7 @@ struct ColKernels {
     int p_smem;
     int p_box_rows;  // rows per 2D TMA box
     int p_tma_m;     // 1: the modulus tile also arrives by TMA
+    int p_threads;   // threads of the pipelined column pass
 };
 RowKernels row_kernels(int N);
 ColKernels col_kernels(int N);

@@ -38,12 +38,12 @@ struct SmemLayout {
 
 // v[i] *= w^i for i = 1..R-1, w = table[t] (conjugated for S > 0); w^2 and
 // w^4 come from the table, the other powers from one product each.
-template <int R, int S>
+template <int R, int S, bool SMEM_TW = false>
 __device__ __forceinline__ void twiddle(float2 *u, const float2 *__restrict__ tw, int t, int n)
 {
     if (t == 0) return;
     auto ld = [&](int idx) {
-        float2 w = __ldg(tw + idx);
+        float2 w = SMEM_TW ? tw[idx] : __ldg(tw + idx);
         if (S > 0) w.y = -w.y;
         return w;
     };
@@ -128,12 +128,13 @@ __device__ __forceinline__ void reg_fft(float2 (&v)[8], float2 *smem, int b, int
 // ---- single-buffer variant with XOR-swizzled layouts -------------------------
 // Used by the pipelined kernels, whose exchange buffer is the TMA stage the
 // data arrived in.  Swizzles chosen by simulating the bank pattern of every
-// exchange (all power-of-two lengths): conflict-free, no padding.
-//  rows:    sequence b at b*N, element e at e ^ ((e >> 4) & 15)
+// exchange (all power-of-two lengths, 8-byte accesses served per half warp):
+// conflict-free, no padding.
+//  rows:    sequence b at b*N, element e at e ^ ((e >> 3) & 15)
 //  columns: element e of sequence b at (e ^ ((e >> 3) & (16/NB - 1)))*NB + b
 template <int N, int NB>
 struct RowSwz {
-    __device__ __forceinline__ static int at(int b, int e) { return b * N + (e ^ ((e >> 4) & 15)); }
+    __device__ __forceinline__ static int at(int b, int e) { return b * N + (e ^ ((e >> 3) & 15)); }
 };
 template <int N, int NB>
 struct ColSwz {
@@ -141,7 +142,132 @@ struct ColSwz {
     __device__ __forceinline__ static int at(int b, int e) { return (e ^ ((e >> 3) & (16 / NB - 1))) * NB + b; }
 };
 
+// ---- per-thread twiddles, loaded once per kernel ----------------------------
+// In pass P (sub-length NS) butterfly i of thread l uses powers of
+// w = tw[((l + i*N/8) mod NS) * N/(NS*R)].  When NS divides N/8 the base does
+// not depend on i, otherwise each of the 8/R butterflies has its own.  A
+// persistent kernel keeps the bases in registers for all its work items and
+// forms w^2..w^7 by products (see twiddle_reg).
+__host__ __device__ constexpr int tw_slots_upto(int N, int P)
+{
+    RadixList L = radix_list(N);
+    int slots = 0, ns = 1;
+    for (int p = 0; p < P && p < L.n; ++p) {
+        if (p > 0) slots += (ns <= N / 8) ? 1 : 8 / L.r[p];
+        ns *= L.r[p];
+    }
+    return slots;
+}
+__host__ __device__ constexpr int tw_slots(int N) { return tw_slots_upto(N, radix_list(N).n); }
+
+template <int N>
+struct RegTw {
+    float2 w[tw_slots(N) > 0 ? tw_slots(N) : 1];
+
+    template <int P, int NS>
+    __device__ __forceinline__ void load_pass(const float2 *__restrict__ tw, int l)
+    {
+        constexpr RadixList L = radix_list(N);
+        if constexpr (P < L.n) {
+            constexpr int R = L.r[P];
+            constexpr int Q = N / 8;
+            if constexpr (P > 0) {
+                constexpr int off = tw_slots_upto(N, P);
+                constexpr int STEP = N / (NS * R);
+                if constexpr (NS <= Q) {
+                    w[off] = __ldg(tw + (l & (NS - 1)) * STEP);
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 8 / R; ++i) w[off + i] = __ldg(tw + ((l + i * Q) & (NS - 1)) * STEP);
+                }
+            }
+            load_pass<P + 1, NS * R>(tw, l);
+        }
+    }
+    __device__ __forceinline__ void load(const float2 *__restrict__ tw, int l) { load_pass<0, 1>(tw, l); }
+};
+
+// u[q] *= w^q, q = 1..R-1, from the base w (conjugated for S > 0).  The
+// empty asm makes the base opaque at each use, so the compiler recomputes
+// the powers instead of hoisting all of them out of the work-item loop
+// (which would keep ~50 more values live per thread).
+template <int R, int S>
+__device__ __forceinline__ void twiddle_reg(float2 *u, float2 w1)
+{
+    asm volatile("" : "+f"(w1.x), "+f"(w1.y));
+    if (S > 0) w1.y = -w1.y;
+    if constexpr (R == 2) {
+        u[1] = cmul(u[1], w1);
+    } else if constexpr (R == 4) {
+        const float2 w2 = cmul(w1, w1);
+        u[1] = cmul(u[1], w1);
+        u[2] = cmul(u[2], w2);
+        u[3] = cmul(u[3], cmul(w1, w2));
+    } else {
+        const float2 w2 = cmul(w1, w1), w4 = cmul(w2, w2);
+        const float2 w3 = cmul(w1, w2);
+        u[1] = cmul(u[1], w1);
+        u[2] = cmul(u[2], w2);
+        u[3] = cmul(u[3], w3);
+        u[4] = cmul(u[4], w4);
+        u[5] = cmul(u[5], cmul(w1, w4));
+        u[6] = cmul(u[6], cmul(w2, w4));
+        u[7] = cmul(u[7], cmul(w3, w4));
+    }
+}
+
 template <int N, class LAYOUT, int S, int P, int NS>
+__device__ __forceinline__ void reg_passes_1buf_rt(float2 (&v)[8], float2 *buf, int b, int l,
+                                                   const RegTw<N> &tw)
+{
+    constexpr RadixList L = radix_list(N);
+    if constexpr (P < L.n) {
+        constexpr int R = L.r[P];
+        constexpr int BPT = 8 / R;
+        constexpr int Q = N / 8;
+        int kk[BPT];
+#pragma unroll
+        for (int i = 0; i < BPT; ++i) {
+            const int j = l + i * Q;
+            const int k = j & (NS - 1);
+            kk[i] = k;
+            float2 u[R];
+#pragma unroll
+            for (int q = 0; q < R; ++q) u[q] = v[i + q * BPT];
+            if constexpr (NS > 1) {
+                constexpr int off = tw_slots_upto(N, P);
+                twiddle_reg<R, S>(u, tw.w[off + (NS <= Q ? 0 : i)]);
+            }
+            dftR<R, S>(u);
+#pragma unroll
+            for (int q = 0; q < R; ++q) v[i + q * BPT] = u[q];
+        }
+        if constexpr (P + 1 < L.n) {
+            __syncthreads();
+#pragma unroll
+            for (int i = 0; i < BPT; ++i) {
+                const int j = l + i * Q;
+                const int base = (j - kk[i]) * R + kk[i];
+#pragma unroll
+                for (int q = 0; q < R; ++q) buf[LAYOUT::at(b, base + q * NS)] = v[i + q * BPT];
+            }
+            __syncthreads();
+#pragma unroll
+            for (int m = 0; m < 8; ++m) v[m] = buf[LAYOUT::at(b, l + m * Q)];
+            reg_passes_1buf_rt<N, LAYOUT, S, P + 1, NS * R>(v, buf, b, l, tw);
+        }
+    }
+}
+
+// As reg_fft_1buf, with the twiddles already in registers.
+template <int N, class LAYOUT, int S>
+__device__ __forceinline__ void reg_fft_1buf(float2 (&v)[8], float2 *buf, int b, int l, const RegTw<N> &tw)
+{
+    static_assert(is_pow2(N) && N >= 16, "pipelined FFT needs a power-of-two length >= 16");
+    reg_passes_1buf_rt<N, LAYOUT, S, 0, 1>(v, buf, b, l, tw);
+}
+
+template <int N, class LAYOUT, int S, int P, int NS, bool SMEM_TW>
 __device__ __forceinline__ void reg_passes_1buf(float2 (&v)[8], float2 *buf, int b, int l,
                                                 const float2 *__restrict__ tw)
 {
@@ -160,7 +286,7 @@ __device__ __forceinline__ void reg_passes_1buf(float2 (&v)[8], float2 *buf, int
             float2 u[R];
 #pragma unroll
             for (int q = 0; q < R; ++q) u[q] = v[i + q * BPT];
-            if constexpr (NS > 1) twiddle<R, S>(u, tw, k * STEP, N);
+            if constexpr (NS > 1) twiddle<R, S, SMEM_TW>(u, tw, k * STEP, N);
             dftR<R, S>(u);
 #pragma unroll
             for (int q = 0; q < R; ++q) v[i + q * BPT] = u[q];
@@ -177,7 +303,7 @@ __device__ __forceinline__ void reg_passes_1buf(float2 (&v)[8], float2 *buf, int
             __syncthreads();
 #pragma unroll
             for (int m = 0; m < 8; ++m) v[m] = buf[LAYOUT::at(b, l + m * Q)];
-            reg_passes_1buf<N, LAYOUT, S, P + 1, NS * R>(v, buf, b, l, tw);
+            reg_passes_1buf<N, LAYOUT, S, P + 1, NS * R, SMEM_TW>(v, buf, b, l, tw);
         }
     }
 }
@@ -185,12 +311,13 @@ __device__ __forceinline__ void reg_passes_1buf(float2 (&v)[8], float2 *buf, int
 // Transform of the sequence in v through one exchange buffer.  Starts every
 // exchange with a barrier (so buf may still be read when it is called) and
 // leaves buf in use: callers synchronise before overwriting it.
-template <int N, class LAYOUT, int S>
+// tw: the length-N twiddle table, in global memory or (SMEM_TW) shared memory.
+template <int N, class LAYOUT, int S, bool SMEM_TW = false>
 __device__ __forceinline__ void reg_fft_1buf(float2 (&v)[8], float2 *buf, int b, int l,
                                              const float2 *__restrict__ tw)
 {
     static_assert(is_pow2(N) && N >= 16, "pipelined FFT needs a power-of-two length >= 16");
-    reg_passes_1buf<N, LAYOUT, S, 0, 1>(v, buf, b, l, tw);
+    reg_passes_1buf<N, LAYOUT, S, 0, 1, SMEM_TW>(v, buf, b, l, tw);
 }
 
 // shared memory (bytes) a register-FFT kernel needs

@@ -838,6 +838,9 @@ __global__ void __launch_bounds__(rrow_threads(N)) k_row_hio_p(const JobDev *job
     __syncthreads();
     int item = next_live(blockIdx.x);
     if (threadIdx.x == 0 && item < n_items) issue(item, 0);
+    // every job of this launch has row length N: one twiddle set for all items
+    RegTw<N> rtw;
+    if (item < n_items) rtw.load(jobs[item_at(L, item).job].prow.tw, l);
     for (int k = 0; item < n_items; ++k) {
         const int nxt = next_live(item + gridDim.x);
         const int s = k & 1;
@@ -865,7 +868,7 @@ __global__ void __launch_bounds__(rrow_threads(N)) k_row_hio_p(const JobDev *job
         float2 v[8];
 #pragma unroll
         for (int m = 0; m < 8; ++m) v[m] = sX[b * N + l + m * Q];
-        reg_fft_1buf<N, RowSwz<N, NB>, +1>(v, sX, b, l, J.prow.tw);
+        reg_fft_1buf<N, RowSwz<N, NB>, +1>(v, sX, b, l, rtw);
         const float beta = J.beta;
         const float thr = st->thr;
         const bool init_gprev = FIRST && st->hio_cycle == 0;
@@ -889,7 +892,7 @@ __global__ void __launch_bounds__(rrow_threads(N)) k_row_hio_p(const JobDev *job
             }
             v[m] = g;
         }
-        reg_fft_1buf<N, RowSwz<N, NB>, -1>(v, sX, b, l, J.prow.tw);
+        reg_fft_1buf<N, RowSwz<N, NB>, -1>(v, sX, b, l, rtw);
         if (ok) {
 #pragma unroll
             for (int m = 0; m < 8; ++m) J.X[base + l + m * Q] = v[m];
@@ -904,13 +907,15 @@ __global__ void __launch_bounds__(rrow_threads(N)) k_row_hio_p(const JobDev *job
 // stage: X tile [N][NB] complex | M tile [N][NB] float (when NB*4 >= 16)
 __host__ __device__ constexpr int pcol_box_rows(int N) { return N < 256 ? N : 256; }
 __host__ __device__ constexpr bool pcol_tma_m(int N) { return rcol_nb(N) * 4 >= 16; }
+__host__ __device__ constexpr int pcol_threads(int N) { return rcol_threads(N); }
 template <int N>
 __host__ __device__ constexpr int pcol_stage_bytes()
 {
     return round128(rcol_nb(N) * N * 8 + (pcol_tma_m(N) ? rcol_nb(N) * N * 4 : 0));
 }
+// barriers | 2 stages | twiddle table (N complex)
 template <int N>
-__host__ __device__ constexpr int pcol_smem() { return 128 + 2 * pcol_stage_bytes<N>(); }
+__host__ __device__ constexpr int pcol_smem() { return 128 + 2 * pcol_stage_bytes<N>() + N * 8; }
 
 template <int N>
 __global__ void __launch_bounds__(rcol_threads(N)) k_col_p(const JobDev *jobs, const WorkList *L)
@@ -933,8 +938,8 @@ __global__ void __launch_bounds__(rcol_threads(N)) k_col_p(const JobDev *jobs, c
     auto issue = [&](int item, int s) {
         const WorkItem wi = item_at(L, item);
         const JobDev &J = jobs[wi.job];
-        const int x0 = wi.tile * NB;
         unsigned char *st = stages + s * STAGE;
+        const int x0 = wi.tile * NB;
         mbar_arrive_expect_tx(&bars[s], (uint32_t)(XB + (TM ? NB * N * 4 : 0)));
         for (int r0 = 0; r0 < N; r0 += BR) {
             tma_load_2d(st + (size_t)r0 * NB * 8, &J.tmX, x0, r0, &bars[s]);
@@ -942,13 +947,20 @@ __global__ void __launch_bounds__(rcol_threads(N)) k_col_p(const JobDev *jobs, c
         }
     };
 
+    // the column length is N for every job of this launch: one twiddle table,
+    // kept in shared memory (the stages leave little L1 for it)
+    float2 *stw = reinterpret_cast<float2 *>(stages + 2 * STAGE);
     if (threadIdx.x == 0) {
         mbar_init(&bars[0], 1);
         mbar_init(&bars[1], 1);
         mbar_fence_init();
     }
-    __syncthreads();
     int item = next_live(blockIdx.x);
+    if (item < n_items) {
+        const float2 *gtw = jobs[item_at(L, item).job].pcol.tw;
+        for (int i = threadIdx.x; i < N; i += rcol_threads(N)) stw[i] = gtw[i];
+    }
+    __syncthreads();
     if (threadIdx.x == 0 && item < n_items) issue(item, 0);
     for (int k = 0; item < n_items; ++k) {
         const int nxt = next_live(item + gridDim.x);
@@ -975,7 +987,7 @@ __global__ void __launch_bounds__(rcol_threads(N)) k_col_p(const JobDev *jobs, c
         float2 v[8];
 #pragma unroll
         for (int m = 0; m < 8; ++m) v[m] = sX[(l + m * Q) * NB + b];
-        reg_fft_1buf<N, ColSwz<N, NB>, -1>(v, sX, b, l, J.pcol.tw);
+        reg_fft_1buf<N, ColSwz<N, NB>, -1, true>(v, sX, b, l, stw);
 #pragma unroll
         for (int m = 0; m < 8; ++m) {
             float mod;
@@ -986,7 +998,7 @@ __global__ void __launch_bounds__(rcol_threads(N)) k_col_p(const JobDev *jobs, c
             const float f = __fdiv_rn(mod, nrm);
             v[m] = make_float2(__fmul_rn(v[m].x, f), __fmul_rn(v[m].y, f));
         }
-        reg_fft_1buf<N, ColSwz<N, NB>, +1>(v, sX, b, l, J.pcol.tw);
+        reg_fft_1buf<N, ColSwz<N, NB>, +1, true>(v, sX, b, l, stw);
         if (ok) {
 #pragma unroll
             for (int m = 0; m < 8; ++m) J.X[(size_t)(l + m * Q) * W + x] = v[m];

@@ -229,7 +229,7 @@ extern "C" int imr_shrink_wrap_noalloc(const float *d_modulus, float *d_out, uns
     const int g_row_first = p_rows ? persistent_grid((const void *)rk.p_hio_first, rk.threads, rk.p_smem_first,
                                                      J.n_row_tiles) : 0;
     const int g_row = p_rows ? persistent_grid((const void *)rk.p_hio, rk.threads, rk.p_smem, J.n_row_tiles) : 0;
-    const int g_col = p_cols ? persistent_grid((const void *)ck.p_col, ck.threads, ck.p_smem, J.n_col_tiles) : 0;
+    const int g_col = p_cols ? persistent_grid((const void *)ck.p_col, ck.p_threads, ck.p_smem, J.n_col_tiles) : 0;
     ck.init<<<J.n_col_tiles, ck.threads, smem_col, s>>>(d_j, d_l + 1);
     for (int c = 0; c <= J.n_cycles; ++c) {
         rk.finish<<<J.n_row_tiles, rk.threads, smem_fin, s>>>(d_j, d_l, nullptr);
@@ -242,7 +242,7 @@ extern "C" int imr_shrink_wrap_noalloc(const float *d_modulus, float *d_out, uns
             } else {
                 (i == 0 ? rk.hio_first : rk.hio)<<<J.n_row_tiles, rk.threads, smem_row, s>>>(d_j, d_l);
             }
-            if (p_cols) ck.p_col<<<g_col, ck.threads, ck.p_smem, s>>>(d_j, d_l + 1);
+            if (p_cols) ck.p_col<<<g_col, ck.p_threads, ck.p_smem, s>>>(d_j, d_l + 1);
             else ck.col<<<J.n_col_tiles, ck.threads, smem_col, s>>>(d_j, d_l + 1);
         }
     }
