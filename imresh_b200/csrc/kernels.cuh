@@ -966,6 +966,7 @@ __global__ void __launch_bounds__(rcol_threads(N)) k_col_p(const JobDev *jobs, c
         const int nxt = next_live(item + gridDim.x);
         const int s = k & 1;
         if (threadIdx.x == 0 && nxt < n_items) {
+            bulk_wait_read0();   // the tile stored from stage s^1 last iteration has left it
             fence_proxy_async_smem();
             issue(nxt, s ^ 1);
         }
@@ -976,6 +977,7 @@ __global__ void __launch_bounds__(rcol_threads(N)) k_col_p(const JobDev *jobs, c
             if (threadIdx.x == 0) {
                 atomicExch(&J.st->err, 1);
                 if (nxt < n_items) mbar_wait(&bars[s ^ 1], (uint32_t)(((k + 1) >> 1) & 1));
+                bulk_wait0();
             }
             return;
         }
@@ -999,14 +1001,20 @@ __global__ void __launch_bounds__(rcol_threads(N)) k_col_p(const JobDev *jobs, c
             v[m] = make_float2(__fmul_rn(v[m].x, f), __fmul_rn(v[m].y, f));
         }
         reg_fft_1buf<N, ColSwz<N, NB>, +1, true>(v, sX, b, l, stw);
-        if (ok) {
+        // the result goes back into the stage (tile layout) and leaves by TMA
+        __syncthreads();
 #pragma unroll
-            for (int m = 0; m < 8; ++m) J.X[(size_t)(l + m * Q) * W + x] = v[m];
-        }
+        for (int m = 0; m < 8; ++m) sX[(l + m * Q) * NB + b] = v[m];
         fence_proxy_async_smem();
         __syncthreads();
+        if (threadIdx.x == 0) {
+            const int x0 = wi.tile * NB;
+            for (int r0 = 0; r0 < N; r0 += BR) tma_store_2d(&J.tmX, x0, r0, sX + (size_t)r0 * NB);
+            bulk_commit();
+        }
         item = nxt;
     }
+    if (threadIdx.x == 0) bulk_wait0();
 }
 
 }  // namespace imr
