@@ -151,31 +151,33 @@ static int admit(imr_engine *E, std::vector<EJob *> &fresh)
     return IMR_SUCCESS;
 }
 
-// Group jobs by the row kernels (width) or the column kernels (height and
-// pipelining), items sorted by the job's HIO count so iteration i runs a
-// prefix of the list.
+// Group jobs by the kernels they run (rows: by width class, columns: by
+// height class and pipelining), so all jobs that share a kernel share its
+// launches -- e.g. every Bluestein width with the same work length.  Items
+// are sorted by the job's HIO count so iteration i runs a prefix of the list.
 static void build_groups(const std::vector<EJob *> &jobs, bool rows, std::vector<Group> &out)
 {
-    std::map<std::pair<int, int>, std::vector<EJob *>> by;
+    std::map<std::pair<const void *, int>, std::vector<EJob *>> by;
     for (EJob *j : jobs) {
-        const int key = rows ? (int)j->W : (int)j->H;
+        const void *key = rows ? (const void *)j->S.rk.hio : (j->S.p_cols ? (const void *)j->S.ck.p_col
+                                                                           : (const void *)j->S.ck.col);
         const int pl = rows ? (j->S.p_rows ? 1 : 0) : (j->S.p_cols ? 1 : 0);
         by[{key, pl}].push_back(j);
     }
     out.clear();
     for (auto &kv : by) {
         Group g;
-        g.key_n = kv.first.first;
-        g.pipelined = kv.first.second != 0;
         auto &v = kv.second;
         std::stable_sort(v.begin(), v.end(), [](EJob *a, EJob *b) { return a->J.n_hio > b->J.n_hio; });
         const EJob *j0 = v.front();
+        g.key_n = rows ? (int)j0->W : (int)j0->H;
+        g.pipelined = kv.first.second != 0;
         g.rk = j0->S.rk;
         g.ck = j0->S.ck;
-        g.smem = rows ? j0->S.smem_row : j0->S.smem_col;
-        g.smem_fin = j0->S.smem_fin;
         int max_hio = 0;
         for (EJob *j : v) {
+            g.smem = std::max(g.smem, rows ? j->S.smem_row : j->S.smem_col);
+            g.smem_fin = std::max(g.smem_fin, j->S.smem_fin);
             const int nt = rows ? j->J.n_row_tiles : j->J.n_col_tiles;
             for (int t = 0; t < nt; ++t) g.items.push_back(WorkItem{j->slot, t});
             max_hio = std::max(max_hio, j->J.n_hio);

@@ -48,15 +48,119 @@ bool factor_len(int n, std::vector<int> &rad)
     return m == 1 && (int)rad.size() <= 14;
 }
 
-// Twiddle tables exp(-2 pi i t/n), t < n, computed in double; one per
-// (device, n), kept for the life of the process.
+// Supported image sides: every length 1..kMaxRuntimeSide (direct mixed-radix
+// transforms when the length factors into 2, 3, 5, 7; Bluestein otherwise),
+// plus the compile-time lengths 3072 and 4096.
+int bluestein_m(int n)
+{
+    int m = 1;
+    while (m < 2 * n - 1) m <<= 1;
+    return m;
+}
+
+bool length_supported(int n)
+{
+    std::vector<int> rad;
+    if (factor_len(n, rad)) return true;
+    return n >= 1 && n <= kMaxRuntimeSide;
+}
+
+// in-place radix-2 FFT in double (host; Bluestein kernel spectra)
+static void host_fft_pow2(std::vector<double> &re, std::vector<double> &im, int sign)
+{
+    const int n = (int)re.size();
+    for (int i = 1, j = 0; i < n; ++i) {
+        int bit = n >> 1;
+        for (; j & bit; bit >>= 1) j ^= bit;
+        j ^= bit;
+        if (i < j) {
+            std::swap(re[i], re[j]);
+            std::swap(im[i], im[j]);
+        }
+    }
+    for (int len = 2; len <= n; len <<= 1) {
+        for (int i = 0; i < n; i += len)
+            for (int k = 0; k < len / 2; ++k) {
+                const double a = sign * 2.0 * M_PI * (double)k / (double)len;
+                const double wr = cos(a), wi = sin(a);
+                const double ur = re[i + k], ui = im[i + k];
+                const double xr = re[i + k + len / 2], xi = im[i + k + len / 2];
+                const double vr = xr * wr - xi * wi, vi = xr * wi + xi * wr;
+                re[i + k] = ur + vr;
+                im[i + k] = ui + vi;
+                re[i + k + len / 2] = ur - vr;
+                im[i + k + len / 2] = ui - vi;
+            }
+    }
+}
+
+// Twiddle tables exp(-2 pi i t/L), t < L, computed in double; one per
+// (device, n), kept for the life of the process.  Bluestein lengths also
+// keep their chirp and kernel spectra in the same allocation.
 static std::mutex g_tw_mu;
 static std::map<std::pair<int, int>, float2 *> g_tw;
+
+static int make_bluestein_plan(int n, FftPlanDev &p)
+{
+    const int M = bluestein_m(n);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(g_tw_mu);
+    auto key = std::make_pair(dev, -n);
+    float2 *d = nullptr;
+    auto it = g_tw.find(key);
+    if (it == g_tw.end()) {
+        std::vector<float2> h((size_t)M + n + 2 * (size_t)M);
+        for (int t = 0; t < M; ++t) {
+            const double a = -2.0 * M_PI * (double)t / (double)M;
+            h[t] = make_float2((float)cos(a), (float)sin(a));
+        }
+        std::vector<double> cre(n), cim(n);
+        for (int j = 0; j < n; ++j) {
+            const long long q = ((long long)j * j) % (2LL * n);   // j^2 mod 2n: exact angle
+            const double a = -M_PI * (double)q / (double)n;
+            cre[j] = cos(a);
+            cim[j] = sin(a);
+            h[M + j] = make_float2((float)cre[j], (float)cim[j]);
+        }
+        for (int dir = 0; dir < 2; ++dir) {   // 0: forward (S = -1), 1: inverse (S = +1)
+            std::vector<double> kr(M, 0.0), ki(M, 0.0);
+            for (int j = 0; j < n; ++j) {
+                // kernel conj(c_j) with c_j = exp(S i pi j^2/n), wrapped for negative j
+                const double br = cre[j], bi = dir == 0 ? -cim[j] : cim[j];
+                kr[j] = br;
+                ki[j] = bi;
+                if (j) {
+                    kr[M - j] = br;
+                    ki[M - j] = bi;
+                }
+            }
+            host_fft_pow2(kr, ki, -1);
+            for (int t = 0; t < M; ++t)
+                h[(size_t)M + n + (size_t)dir * M + t] = make_float2((float)(kr[t] / M), (float)(ki[t] / M));
+        }
+        cudaError_t e = cudaMalloc(&d, sizeof(float2) * h.size());
+        if (e != cudaSuccess) { set_error("cudaMalloc Bluestein tables", e); return IMR_ERR_OUT_OF_MEMORY; }
+        e = cudaMemcpy(d, h.data(), sizeof(float2) * h.size(), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) { set_error("cudaMemcpy Bluestein tables", e); return IMR_ERR_CUDA; }
+        g_tw[key] = d;
+    } else {
+        d = it->second;
+    }
+    memset(&p, 0, sizeof(p));
+    p.n = n;
+    p.bs_m = M;
+    p.tw = d;
+    p.chirp = d + M;
+    p.bspec_f = d + M + n;
+    p.bspec_b = d + M + n + M;
+    return IMR_SUCCESS;
+}
 
 int make_fft_plan(int n, FftPlanDev &p)
 {
     std::vector<int> rad;
-    if (!factor_len(n, rad)) return IMR_ERR_UNSUPPORTED_SIZE;
+    if (!factor_len(n, rad)) return length_supported(n) ? make_bluestein_plan(n, p) : IMR_ERR_UNSUPPORTED_SIZE;
     int dev = 0;
     cudaGetDevice(&dev);
     std::lock_guard<std::mutex> lk(g_tw_mu);
@@ -115,14 +219,15 @@ static RowKernels row_set()
         return RowKernels{k_row_hio_r<true, N>, k_row_hio_r<false, N>, k_row_finish_r<N>,
                           k_fft_rows_r<-1, N>, k_fft_rows_r<+1, N>, rrow_nb(N), rrow_threads(N),
                           rrow_smem(N), k_row_hio_p<true, N>, k_row_hio_p<false, N>,
-                          prow_smem<true, N>(), prow_smem<false, N>()};
+                          prow_smem<true, N>(), prow_smem<false, N>(), 0};
     else if constexpr (N >= 8 && is_pow2(N))
         return RowKernels{k_row_hio_r<true, N>, k_row_hio_r<false, N>, k_row_finish_r<N>,
                           k_fft_rows_r<-1, N>, k_fft_rows_r<+1, N>, rrow_nb(N), rrow_threads(N),
-                          rrow_smem(N), nullptr, nullptr, 0, 0};
+                          rrow_smem(N), nullptr, nullptr, 0, 0, 0};
     else
         return RowKernels{k_row_hio<true, N>, k_row_hio<false, N>, k_row_finish<N>, k_fft_rows<-1, N>,
-                          k_fft_rows<+1, N>, row_nb(N), row_threads(N), 0, nullptr, nullptr, 0, 0};
+                          k_fft_rows<+1, N>, row_nb(N), row_threads(N), 0, nullptr, nullptr, 0, 0,
+                          N < 0 ? -N : 0};
 }
 template <int N>
 static ColKernels col_set()
@@ -130,13 +235,13 @@ static ColKernels col_set()
     if constexpr (N >= 16 && is_pow2(N))
         return ColKernels{k_col_r<N>, k_col_init_r<N>, k_fft_cols_r<-1, N>, k_fft_cols_r<+1, N>,
                           rcol_nb(N), rcol_threads(N), rcol_smem(N), k_col_p<N>, pcol_smem<N>(),
-                          pcol_box_rows(N), pcol_tma_m(N) ? 1 : 0, pcol_threads(N)};
+                          pcol_box_rows(N), pcol_tma_m(N) ? 1 : 0, pcol_threads(N), 0};
     else if constexpr (N >= 8 && is_pow2(N))
         return ColKernels{k_col_r<N>, k_col_init_r<N>, k_fft_cols_r<-1, N>, k_fft_cols_r<+1, N>,
-                          rcol_nb(N), rcol_threads(N), rcol_smem(N), nullptr, 0, 0, 0, 0};
+                          rcol_nb(N), rcol_threads(N), rcol_smem(N), nullptr, 0, 0, 0, 0, 0};
     else
         return ColKernels{k_col<N>, k_col_init<N>, k_fft_cols<-1, N>, k_fft_cols<+1, N>, col_nb(N),
-                          col_threads(N), 0, nullptr, 0, 0, 0, 0};
+                          col_threads(N), 0, nullptr, 0, 0, 0, 0, N < 0 ? -N : 0};
 }
 
 int persistent_grid(const void *kernel, int threads, int smem, int items)
@@ -177,12 +282,17 @@ bool encode_tensor_map(CUtensorMap *map, const void *base, int W, int H, int ele
 }
 
 #define IMR_SIZES(X) X(64) X(128) X(192) X(256) X(384) X(512) X(768) X(1024) X(1536) X(2048) X(3072) X(4096)
+// Bluestein transform lengths M (power of two >= 2n - 1 for n <= 2048)
+#define IMR_BS_SIZES(X) X(-8) X(-16) X(-32) X(-64) X(-128) X(-256) X(-512) X(-1024) X(-2048) X(-4096)
 
 RowKernels row_kernels(int N)
 {
+    std::vector<int> rad;
+    if (!factor_len(N, rad) && length_supported(N)) N = -bluestein_m(N);
     switch (N) {
 #define ROWCASE(n) case n: return row_set<n>();
         IMR_SIZES(ROWCASE)
+        IMR_BS_SIZES(ROWCASE)
 #undef ROWCASE
     default: {
         RowKernels k = row_set<0>();
@@ -195,9 +305,12 @@ RowKernels row_kernels(int N)
 
 ColKernels col_kernels(int N)
 {
+    std::vector<int> rad;
+    if (!factor_len(N, rad) && length_supported(N)) N = -bluestein_m(N);
     switch (N) {
 #define COLCASE(n) case n: return col_set<n>();
         IMR_SIZES(COLCASE)
+        IMR_BS_SIZES(COLCASE)
 #undef COLCASE
     default: {
         ColKernels k = col_set<0>();
@@ -238,9 +351,18 @@ int ensure_kernel_attributes()
 #define PUSH(n) sizes.push_back(n);
     IMR_SIZES(PUSH)
 #undef PUSH
+    std::vector<RowKernels> rks;
+    std::vector<ColKernels> cks;
     for (int n : sizes) {
-        RowKernels r = n ? row_kernels(n) : row_set<0>();
-        ColKernels c = n ? col_kernels(n) : col_set<0>();
+        rks.push_back(n ? row_kernels(n) : row_set<0>());
+        cks.push_back(n ? col_kernels(n) : col_set<0>());
+    }
+#define PUSHBS(n) rks.push_back(row_set<n>()); cks.push_back(col_set<n>());
+    IMR_BS_SIZES(PUSHBS)
+#undef PUSHBS
+    for (size_t q = 0; q < rks.size(); ++q) {
+        RowKernels r = rks[q];
+        ColKernels c = cks[q];
         if (e == cudaSuccess) e = allow_smem(r.hio_first);
         if (e == cudaSuccess) e = allow_smem(r.hio);
         if (e == cudaSuccess) e = allow_smem(r.finish);
@@ -394,11 +516,15 @@ int job_prepare(unsigned W, unsigned H, const imr_params &p, JobDev &J, JobShape
     // the image has fewer rows / columns than NB
     if (S.rk.smem) {
         S.smem_row = S.smem_fin = (size_t)S.rk.smem;   // norms reuse the FFT buffers
+    } else if (S.rk.bs_m) {   // row + Bluestein work area (the norms reuse the work area)
+        S.smem_row = S.smem_fin = ((size_t)J.W + S.rk.bs_m) * sizeof(float2);
     } else {
         S.smem_row = (size_t)S.rk.nb * J.W * sizeof(float2);
         S.smem_fin = S.smem_row + (size_t)S.rk.nb * J.W * sizeof(float);
     }
-    S.smem_col = S.ck.smem ? (size_t)S.ck.smem : (size_t)S.ck.nb * J.H * sizeof(float2);
+    S.smem_col = S.ck.smem ? (size_t)S.ck.smem
+                 : S.ck.bs_m ? ((size_t)J.H + S.ck.bs_m) * S.ck.nb * sizeof(float2)
+                             : (size_t)S.ck.nb * J.H * sizeof(float2);
     const size_t N = (size_t)W * H;
     auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
     size_t off = 0;
@@ -478,11 +604,7 @@ const char *imr_last_error(void) { return g_last_error; }
 
 unsigned imr_max_side(void) { return kMaxSide; }
 
-int imr_side_supported(unsigned n)
-{
-    std::vector<int> r;
-    return factor_len((int)n, r) ? 1 : 0;
-}
+int imr_side_supported(unsigned n) { return length_supported((int)n) ? 1 : 0; }
 
 int imr_gaussian_weights(double sigma, float *h_w, int cap)
 {
@@ -737,8 +859,8 @@ int imr_fft2d(void *d_data, unsigned W, unsigned H, int sign, void *stream)
     cudaStream_t s = (cudaStream_t)stream;
     float2 *d = (float2 *)d_data;
     const int nrt = ((int)H + rpc - 1) / rpc, nct = ((int)W + cpc - 1) / cpc;
-    const size_t sr = rk.smem ? (size_t)rk.smem : (size_t)rpc * W * 8;
-    const size_t sc = ck.smem ? (size_t)ck.smem : (size_t)cpc * H * 8;
+    const size_t sr = rk.smem ? (size_t)rk.smem : ((size_t)rpc * W + rk.bs_m) * 8;
+    const size_t sc = ck.smem ? (size_t)ck.smem : ((size_t)H + ck.bs_m) * cpc * 8;
     if (sign < 0) {
         rk.fft_fwd<<<nrt, rk.threads, sr, s>>>(d, pr, (int)H, rpc);
         ck.fft_fwd<<<nct, ck.threads, sc, s>>>(d, pc, (int)W, cpc);
@@ -776,8 +898,7 @@ int imr_gaussian_blur(float *d_data, float *d_tmp, unsigned W, unsigned H, doubl
 int imr_diffraction_intensity(float *h_io, unsigned W, unsigned H, void *stream)
 {
     if (!h_io || W == 0 || H == 0) return IMR_ERR_INVALID_VALUE;
-    std::vector<int> r;
-    if (!factor_len((int)W, r) || !factor_len((int)H, r)) return IMR_ERR_UNSUPPORTED_SIZE;
+    if (!length_supported((int)W) || !length_supported((int)H)) return IMR_ERR_UNSUPPORTED_SIZE;
     cudaStream_t s = (cudaStream_t)stream;
     const size_t N = (size_t)W * H;
     float2 *d = nullptr;

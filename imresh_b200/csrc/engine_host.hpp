@@ -13,6 +13,8 @@ constexpr int kMaxRuntimeSide = 2048;
 extern thread_local char g_last_error[256];   // imr_last_error() text
 void set_error(const char *what, cudaError_t e);
 bool factor_len(int n, std::vector<int> &rad);
+bool length_supported(int n);
+int bluestein_m(int n);
 int make_fft_plan(int n, FftPlanDev &p);
 int gaussian_weights(double sigma, float *w, int cap);
 int ensure_kernel_attributes();
@@ -33,6 +35,7 @@ struct RowKernels {
     void (*p_hio_first)(const JobDev *, const WorkList *);
     void (*p_hio)(const JobDev *, const WorkList *);
     int p_smem_first, p_smem;
+    int bs_m;      // Bluestein work length (0: direct transform)
 };
 // Kernels and launch shape of the column passes for one column length.
 struct ColKernels {
@@ -48,6 +51,7 @@ struct ColKernels {
     int p_box_rows;  // rows per 2D TMA box
     int p_tma_m;     // 1: the modulus tile also arrives by TMA
     int p_threads;   // threads of the pipelined column pass
+    int bs_m;        // Bluestein work length (0: direct transform)
 };
 RowKernels row_kernels(int N);
 ColKernels col_kernels(int N);

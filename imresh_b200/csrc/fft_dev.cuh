@@ -27,7 +27,13 @@ struct FftPlanDev {
     int n;           // transform length
     int nrad;        // number of radix passes
     int rad[14];     // radices, first pass first
-    const float2 *tw;  // n entries: exp(-2*pi*i*t/n), computed in double on the host
+    const float2 *tw;  // exp(-2*pi*i*t/L), t < L, computed in double on the host; L = n, or bs_m
+    // Bluestein (lengths with a prime factor > 7): the length-n DFT runs as a
+    // convolution on the power-of-two length bs_m >= 2n - 1
+    int bs_m;                // 0: direct transform
+    const float2 *chirp;     // n entries: exp(-i*pi*j^2/n)
+    const float2 *bspec_f;   // bs_m entries: FFT of the kernel for forward transforms, / bs_m
+    const float2 *bspec_b;   // bs_m entries: the same for inverse transforms
 };
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b)
@@ -300,6 +306,56 @@ __device__ __forceinline__ void ct_fft(float2 *buf, int nb, const float2 *__rest
 {
     static_assert(radix_list(N).n > 0, "length must factor into 2, 3, 5, 7");
     ct_passes<N, NB, T, S, SEQ_FAST, 0, 1>(buf, nb, tw);
+}
+
+// ---- Bluestein -------------------------------------------------------------
+// X[k] = c_k * sum_j (x_j c_j) conj(c_{k-j}),  c_j = exp(S*i*pi*j^2/n)
+//      = c_k * IFFT_M( FFT_M(a) * FFT_M(b) )[k],  a_j = x_j c_j (zero padded),
+// b the kernel conj(c_j) wrapped on the M grid; FFT_M(b)/M is precomputed
+// (bspec_f for S = -1, bspec_b for S = +1).  nb sequences: data element
+// (b, j) at b*dbs + j*des, work element (b, j) at the compile-time layout of
+// ct_fft<M, NB, T, ., SEQ_FAST>.  Ends with a barrier.
+template <int M, int NB, int T, int S, bool SEQ_FAST>
+__device__ __forceinline__ void bluestein(float2 *data, int dbs, int des, float2 *work, int nb,
+                                          const FftPlanDev &p)
+{
+    const int n = p.n;
+    constexpr int WBS = SEQ_FAST ? 1 : M;
+    constexpr int WES = SEQ_FAST ? NB : 1;
+    for (int idx = threadIdx.x; idx < NB * M; idx += T) {
+        int b, j;
+        if (SEQ_FAST) { b = idx % NB; j = idx / NB; }
+        else          { j = idx % M;  b = idx / M; }
+        float2 v = make_float2(0.f, 0.f);
+        if (b < nb && j < n) {
+            float2 c = __ldg(p.chirp + j);
+            if (S > 0) c.y = -c.y;
+            v = cmul(data[b * dbs + j * des], c);
+        }
+        work[b * WBS + j * WES] = v;
+    }
+    __syncthreads();
+    ct_fft<M, NB, T, -1, SEQ_FAST>(work, nb, p.tw);
+    const float2 *spec = S < 0 ? p.bspec_f : p.bspec_b;
+    for (int idx = threadIdx.x; idx < NB * M; idx += T) {
+        int b, j;
+        if (SEQ_FAST) { b = idx % NB; j = idx / NB; }
+        else          { j = idx % M;  b = idx / M; }
+        work[b * WBS + j * WES] = cmul(work[b * WBS + j * WES], __ldg(spec + j));
+    }
+    __syncthreads();
+    ct_fft<M, NB, T, +1, SEQ_FAST>(work, nb, p.tw);
+    for (int idx = threadIdx.x; idx < NB * n; idx += T) {
+        int b, j;
+        if (SEQ_FAST) { b = idx % NB; j = idx / NB; }
+        else          { j = idx % n;  b = idx / n; }
+        if (b < nb) {
+            float2 c = __ldg(p.chirp + j);
+            if (S > 0) c.y = -c.y;
+            data[b * dbs + j * des] = cmul(work[b * WBS + j * WES], c);
+        }
+    }
+    __syncthreads();
 }
 
 // Full transform of nb sequences held in shared memory (see layout above).

@@ -51,27 +51,47 @@ __device__ __forceinline__ WorkItem item_at(const WorkList *L, int i)
 // Row passes: NB rows of length N per CTA, T threads.  Column passes: NB
 // columns of length N per CTA (one tile row = NB contiguous complex values),
 // T threads.  N = 0 selects the runtime-length FFT.
-__host__ __device__ constexpr int row_nb(int N) { return N == 0 ? 0 : (N <= 2048 ? 2048 / N : 1); }
-__host__ __device__ constexpr int row_threads(int N) { return N == 0 ? kRowThreads : 256; }
-__host__ __device__ constexpr int col_nb(int N) { return N == 0 ? 0 : (N <= 2048 ? 8 : 4); }
+// N < 0: Bluestein on the power-of-two length M = -N (one row per CTA;
+// column tiles of 8192/M columns).
+__host__ __device__ constexpr int row_nb(int N) { return N == 0 ? 0 : (N < 0 ? 1 : (N <= 2048 ? 2048 / N : 1)); }
+__host__ __device__ constexpr int row_threads(int N)
+{
+    return N == 0 ? kRowThreads : (N < 0 ? (-N / 8 < 64 ? 64 : -N / 8) : 256);
+}
+__host__ __device__ constexpr int col_nb(int N)
+{
+    return N == 0 ? 0 : (N < 0 ? (8192 / -N > 8 ? 8 : (8192 / -N < 1 ? 1 : 8192 / -N)) : (N <= 2048 ? 8 : 4));
+}
+__host__ __device__ constexpr int col_len(int N) { return N < 0 ? -N : N; }
 __host__ __device__ constexpr int col_threads(int N)
 {
     return N == 0 ? kColThreads
-                  : ((col_nb(N) * N / 16 + 31) / 32 * 32 < 64 ? 64
-                     : ((col_nb(N) * N / 16 + 31) / 32 * 32 > 1024 ? 1024 : (col_nb(N) * N / 16 + 31) / 32 * 32));
+                  : ((col_nb(N) * col_len(N) / 16 + 31) / 32 * 32 < 64 ? 64
+                     : ((col_nb(N) * col_len(N) / 16 + 31) / 32 * 32 > 1024
+                            ? 1024
+                            : (col_nb(N) * col_len(N) / 16 + 31) / 32 * 32));
 }
 
+// Rows in shared memory at b*n + e; a Bluestein transform works in the
+// region after the row_nb(N) rows (M complex per row).
 template <int N, int S>
 __device__ __forceinline__ void fft_rows(float2 *sm, int nr, const FftPlanDev &p)
 {
     if constexpr (N > 0) ct_fft<N, row_nb(N), row_threads(N), S, false>(sm, nr, p.tw);
+    else if constexpr (N < 0)
+        bluestein<-N, 1, row_threads(N), S, false>(sm, p.n, 1, sm + (size_t)row_nb(N) * p.n, nr, p);
     else fft_smem<S, kRowVpt>(sm, p, nr, p.n, 1, false, threadIdx.x, kRowThreads);
 }
 
+// Column tiles in shared memory at e*col_nb(N) + b; a Bluestein transform
+// works in the region after the tile (M * col_nb(N) complex).
 template <int N, int S>
 __device__ __forceinline__ void fft_cols(float2 *sm, int nc, const FftPlanDev &p)
 {
     if constexpr (N > 0) ct_fft<N, col_nb(N), col_threads(N), S, true>(sm, nc, p.tw);
+    else if constexpr (N < 0)
+        bluestein<-N, col_nb(N), col_threads(N), S, true>(sm, 1, col_nb(N), sm + (size_t)col_nb(N) * p.n, nc,
+                                                          p);
     else fft_smem<S, kColVpt>(sm, p, nc, 1, nc, true, threadIdx.x, kColThreads);
 }
 
@@ -183,7 +203,7 @@ __device__ __forceinline__ void b_col_init(const JobDev *jobs, const WorkItem wi
     const int x0 = wi.tile * J.cpc;
     const int nc = min(J.cpc, W - x0);
     constexpr int T = col_threads(N);
-    const int es = N > 0 ? col_nb(N) : nc;   // smem row stride of the tile
+    const int es = N != 0 ? col_nb(N) : nc;   // smem row stride of the tile
     for (int i = threadIdx.x; i < H * nc; i += T) {
         const int y = i / nc, c = i - y * nc;
         sm[y * es + c] = make_float2(J.M[(size_t)y * W + x0 + c], 0.f);
@@ -216,7 +236,7 @@ __device__ __forceinline__ void b_col(const JobDev *jobs, const WorkItem wi)
     const int x0 = wi.tile * J.cpc;
     const int nc = min(J.cpc, W - x0);
     constexpr int T = col_threads(N);
-    const int es = N > 0 ? col_nb(N) : nc;
+    const int es = N != 0 ? col_nb(N) : nc;
     for (int i = threadIdx.x; i < H * nc; i += T) {
         const int y = i / nc, c = i - y * nc;
         sm[y * es + c] = J.X[(size_t)y * W + x0 + c];
@@ -449,7 +469,7 @@ __global__ void __launch_bounds__(col_threads(N)) k_fft_cols(float2 *data, FftPl
     const int H = p.n;
     const int x0 = blockIdx.x * cpc;
     const int nc = min(cpc, W - x0);
-    const int es = N > 0 ? col_nb(N) : nc;
+    const int es = N != 0 ? col_nb(N) : nc;
     for (int i = threadIdx.x; i < H * nc; i += T) {
         const int y = i / nc, c = i - y * nc;
         sm[y * es + c] = data[(size_t)y * W + x0 + c];

@@ -58,8 +58,9 @@ const char *imr_status_string(int status);
 const char *imr_last_error(void);
 
 /* Largest supported image side and whether a side length is supported:
- * lengths whose prime factors are all in {2, 3, 5, 7}, from 1 to 2048, plus
- * 3072 and 4096. */
+ * every length from 1 to 2048 (direct mixed-radix transforms for lengths
+ * whose prime factors are all in {2, 3, 5, 7}, Bluestein's chirp-z transform
+ * otherwise), plus 3072 and 4096. */
 unsigned imr_max_side(void);
 int imr_side_supported(unsigned n);
 

@@ -28,8 +28,8 @@ def test_status_strings():
 
 @pytest.mark.parametrize("n,ok", [(1, True), (2, True), (64, True), (192, True), (210, True),
                                   (343, True), (4096, True), (3072, True), (2187, False), (2400, False),
-                                  (2048, True), (4097, False), (11, False),
-                                  (1031, False), (0, False), (8192, False)])
+                                  (2048, True), (4097, False), (11, True), (1031, True), (2039, True),
+                                  (0, False), (8192, False), (2049, False)])
 def test_side_supported(n, ok):
     assert imr.side_supported(n) == ok
     assert imr.lib().imr_max_side() == 4096

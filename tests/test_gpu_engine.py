@@ -17,6 +17,7 @@ FLT_MIN = imr.FLT_MIN
 MIX = [  # (W, H, cycles, hio)
     (128, 128, 3, 5), (192, 256, 2, 4), (256, 192, 4, 3), (384, 128, 2, 5), (512, 512, 3, 2),
     (96, 64, 3, 4), (256, 256, 1, 6), (128, 384, 2, 5), (160, 120, 2, 3), (64, 64, 5, 2),
+    (100, 97, 2, 4), (131, 77, 2, 3), (97, 100, 3, 2),   # Bluestein widths / heights
 ]
 
 

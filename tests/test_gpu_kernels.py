@@ -18,7 +18,9 @@ FLT_EPS = float(np.finfo(np.float32).eps)
 
 FFT_SHAPES = [(256, 256), (2048, 2048), (128, 384), (384, 192), (512, 128), (64, 64),
               (7, 5), (1, 64), (64, 1), (210, 343), (3, 1536), (4096, 4096), (1024, 768),
-              (100, 90)]
+              (100, 90),
+              # Bluestein lengths (a prime factor > 7)
+              (97, 101), (11, 64), (1031, 7), (64, 2039), (257, 300), (13, 13), (2047, 2)]
 
 
 def _to_dev(a):

@@ -41,7 +41,8 @@ def _run_gpu(M, p: oracle.SwParams, cuda_defaults=False):
     return out, n, errs, mask
 
 
-@pytest.mark.parametrize("shape", [(64, 64), (256, 256), (128, 384), (192, 512), (2048, 2048)])
+@pytest.mark.parametrize("shape", [(64, 64), (256, 256), (128, 384), (192, 512), (2048, 2048),
+                                   (97, 130), (211, 64)])
 def test_one_cycle_matches_oracle(cuda, shape):
     H, W = shape
     M, _ = data.make_modulus(_spec(W, H), 1)
@@ -124,7 +125,7 @@ def test_reference_cuda_defaults(cuda):
 
 def test_unsupported_size_is_an_error(cuda):
     with pytest.raises(imr.ImrError) as e:
-        imr.Plan(11, 64)
+        imr.Plan(2500, 64)
     assert e.value.status == 2
     io = np.zeros(4097 * 2, np.float32)
     assert imr.cuda_shrink_wrap(io, 4097, 2) == 2
