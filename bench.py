@@ -103,6 +103,118 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def _lat_stats(lat_ms):
+    lat = np.sort(np.asarray(lat_ms, dtype=np.float64))
+    return float(np.percentile(lat, 50)), float(np.percentile(lat, 99))
+
+
+def run_batched(n_jobs: int = 512, plain_sample: int = 64):
+    """The uneven batch: n_jobs reconstructions, W and H each from
+    {128,192,256,384,512}, 20-200 blobs, Poisson 1e7-1e9 photons, seed 2,
+    64 cycles x 20 HIO.  Served by the batched engine (all jobs submitted at
+    once, host buffers, copies included) vs the plain path (one plan per
+    shape, one reconstruction at a time, host buffers) on a sample of the
+    same jobs.  Both wall-clock timed around synchronous calls."""
+    import imresh_b200 as imr
+    from imresh_b200 import data
+    specs = data.cfg2_specs(n_jobs, seed=2)
+    inputs = [data.make_modulus(sp, seed=2, index=i)[0] for i, sp in enumerate(specs)]
+    prm = imr.Params(64, imr.FLT_MIN, 0.9, 0.04, 0.2, 3.0, 0.01, 20)
+    # warm-up: one small job of every shape class through the engine
+    eng = imr.Engine()
+    for i, M in enumerate(inputs[:8]):
+        eng.submit(M, imr.Params(1, imr.FLT_MIN, 0.9, 0.04, 0.2, 3.0, 0.01, 1), tag=i)
+    eng.run()
+    eng.poll()
+    t0 = time.perf_counter()
+    for i, M in enumerate(inputs):
+        eng.submit(M, prm, tag=i)
+    eng.run()
+    dt = time.perf_counter() - t0
+    res = eng.poll(n_jobs)
+    info = eng.info()
+    eng.close()
+    assert len(res) == n_jobs and all(r["status"] == 0 for r in res)
+    p50, p99 = _lat_stats([r["latency_ms"] for r in res])
+    # plain path on the first plain_sample jobs
+    plans = {}
+    for M in inputs[:plain_sample]:
+        key = M.shape
+        if key not in plans:
+            plans[key] = imr.Plan(M.shape[1], M.shape[0], prm)
+            plans[key].execute_host(M)   # warm
+    lat = []
+    t1 = time.perf_counter()
+    for M in inputs[:plain_sample]:
+        a = time.perf_counter()
+        plans[M.shape].execute_host(M)
+        lat.append((time.perf_counter() - a) * 1e3)
+    dt_plain = time.perf_counter() - t1
+    for p in plans.values():
+        p.close()
+    px = sum(M.size for M in inputs)
+    return {
+        "workload": f"{n_jobs} uneven reconstructions, W,H in {{128..512}}, 64 cycles x 20 HIO, "
+                    "Poisson 1e7-1e9, seed 2",
+        "engine_recon_per_s": n_jobs / dt, "engine_seconds": dt,
+        "engine_hio_iterations_per_s": n_jobs * 64 * 20 / dt,
+        "engine_gbs_algorithmic": px * 64 * 20 * 53 / dt / 1e9,
+        "engine_latency_p50_ms": p50, "engine_latency_p99_ms": p99,
+        "engine_device_bytes_peak": info["device_bytes_peak"], "engine_launches": info["launches"],
+        "plain_recon_per_s": plain_sample / dt_plain, "plain_sample_jobs": plain_sample,
+        "plain_latency_p50_ms": _lat_stats(lat)[0],
+        "speedup_engine_vs_plain": (n_jobs / dt) / (plain_sample / dt_plain),
+        "timing": "wall clock around synchronous calls; host buffers, copies included",
+    }
+
+
+def run_served(n_req: int, rate_hz: float, seed: int = 4, max_side: int = 2048):
+    """Serving stream: n_req requests with Poisson arrivals at rate_hz;
+    W, H log-uniform integers in [64, max_side] (any length: mixed radix or
+    Bluestein), 0.5-3 blobs per 1000 px^2, Poisson 1e6-1e9 photons; each
+    request stops at error 1e-5 or 128 cycles.  Requests are admitted by the
+    engine between steps as device memory allows; latency = arrival ->
+    result in host memory."""
+    import imresh_b200 as imr
+    from imresh_b200 import data
+    specs = data.cfg4_specs(n_req, seed=seed)
+    for sp in specs:
+        sp.width = min(sp.width, max_side)
+        sp.height = min(sp.height, max_side)
+    inputs = [data.make_modulus(sp, seed=seed, index=i)[0] for i, sp in enumerate(specs)]
+    rng = np.random.default_rng([seed, 7])
+    arrivals = np.cumsum(rng.exponential(1.0 / rate_hz, n_req))
+    prm = imr.Params(128, 1e-5, 0.9, 0.04, 0.2, 3.0, 0.01, 20)
+    eng = imr.Engine()
+    done, nxt, lat, t0 = 0, 0, [], time.perf_counter()
+    submit_t = {}
+    peak_active = 0
+    while done < n_req:
+        now = time.perf_counter() - t0
+        while nxt < n_req and arrivals[nxt] <= now:
+            eng.submit(inputs[nxt], prm, tag=nxt)
+            submit_t[nxt] = t0 + arrivals[nxt]
+            nxt += 1
+        info = eng.info()
+        peak_active = max(peak_active, info["active"])
+        if info["active"] == 0 and info["pending"] == 0:
+            time.sleep(max(0.0, min(0.01, arrivals[nxt] - now)) if nxt < n_req else 0)
+            continue
+        eng.step()
+        for r in eng.poll():
+            lat.append((time.perf_counter() - submit_t[r["tag"]]) * 1e3)
+            done += 1
+    wall = time.perf_counter() - t0
+    info = eng.info()
+    eng.close()
+    p50, p99 = _lat_stats(lat)
+    return {"workload": f"{n_req} requests, Poisson arrivals at {rate_hz} /s, sides log-uniform "
+                        f"64..{max_side}, stop at 1e-5 or 128 cycles, seed {seed}",
+            "recon_per_s": n_req / wall, "latency_p50_ms": p50, "latency_p99_ms": p99,
+            "peak_active": peak_active, "device_bytes_peak": info["device_bytes_peak"],
+            "steps": info["steps"], "launches": info["launches"]}
+
+
 def make_input():
     from imresh_b200 import data
     M, _ = data.make_modulus(data.cfg1_spec(), seed=1)
@@ -296,6 +408,8 @@ def run_ours(args, rank, world, local_rank):
     }
     if cpu is not None:
         out["cpu_baseline"] = cpu
+    if world == 1 and not args.no_batched:
+        out["batched"] = run_batched()
     print(json.dumps(out), flush=True)
 
 
@@ -306,7 +420,16 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the uneven-batch comparison")
+    ap.add_argument("--serve", type=int, default=0, metavar="N",
+                    help="only run the serving stream with N requests and print its JSON")
+    ap.add_argument("--rate", type=float, default=20.0, help="serving arrival rate, requests/s")
     args = ap.parse_args()
+    if args.serve:
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps(run_served(args.serve, args.rate)), flush=True)
+        return
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))

@@ -224,6 +224,10 @@ static RowKernels row_set()
         return RowKernels{k_row_hio_r<true, N>, k_row_hio_r<false, N>, k_row_finish_r<N>,
                           k_fft_rows_r<-1, N>, k_fft_rows_r<+1, N>, rrow_nb(N), rrow_threads(N),
                           rrow_smem(N), nullptr, nullptr, 0, 0, 0};
+    else if constexpr (is_3pow2(N))   // per-tile kernels + pipelined 12-value register passes
+        return RowKernels{k_row_hio<true, N>, k_row_hio<false, N>, k_row_finish<N>, k_fft_rows<-1, N>,
+                          k_fft_rows<+1, N>, row_nb(N), row_threads(N), 0, k_row_hio_p<true, N>,
+                          k_row_hio_p<false, N>, prow_smem<true, N>(), prow_smem<false, N>(), 0};
     else
         return RowKernels{k_row_hio<true, N>, k_row_hio<false, N>, k_row_finish<N>, k_fft_rows<-1, N>,
                           k_fft_rows<+1, N>, row_nb(N), row_threads(N), 0, nullptr, nullptr, 0, 0,
@@ -239,6 +243,10 @@ static ColKernels col_set()
     else if constexpr (N >= 8 && is_pow2(N))
         return ColKernels{k_col_r<N>, k_col_init_r<N>, k_fft_cols_r<-1, N>, k_fft_cols_r<+1, N>,
                           rcol_nb(N), rcol_threads(N), rcol_smem(N), nullptr, 0, 0, 0, 0, 0};
+    else if constexpr (is_3pow2(N))
+        return ColKernels{k_col<N>, k_col_init<N>, k_fft_cols<-1, N>, k_fft_cols<+1, N>, col_nb(N),
+                          col_threads(N), 0, k_col_p<N>, pcol_smem<N>(), pcol_box_rows(N),
+                          pcol_tma_m(N) ? 1 : 0, pcol_threads(N), 0};
     else
         return ColKernels{k_col<N>, k_col_init<N>, k_fft_cols<-1, N>, k_fft_cols<+1, N>, col_nb(N),
                           col_threads(N), 0, nullptr, 0, 0, 0, 0, N < 0 ? -N : 0};

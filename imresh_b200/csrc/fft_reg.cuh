@@ -20,6 +20,22 @@ namespace imr {
 
 __host__ __device__ constexpr bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
 
+// Lengths the pipelined register FFT handles: powers of two (8 values per
+// thread, radices 8/4/2) and 3 * 2^k (12 values per thread, radices 4/2/3).
+__host__ __device__ constexpr bool is_3pow2(int n) { return n >= 48 && n % 3 == 0 && is_pow2(n / 3); }
+__host__ __device__ constexpr int reg_v(int n) { return is_pow2(n) ? 8 : 12; }
+__host__ __device__ constexpr RadixList reg_radix_list(int n)
+{
+    if (is_pow2(n)) return radix_list(n);
+    RadixList L{0, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0}};
+    int k = 0, m = n / 3;
+    while (m > 1) { m >>= 1; ++k; }
+    for (; k >= 2; k -= 2) L.r[L.n++] = 4;
+    if (k == 1) L.r[L.n++] = 2;
+    L.r[L.n++] = 3;
+    return L;
+}
+
 // padded index of element e
 __device__ __forceinline__ int pad8(int e) { return e + (e >> 3); }
 
@@ -50,6 +66,9 @@ __device__ __forceinline__ void twiddle(float2 *u, const float2 *__restrict__ tw
     const float2 w1 = ld(t);
     if constexpr (R == 2) {
         u[1] = cmul(u[1], w1);
+    } else if constexpr (R == 3) {
+        u[1] = cmul(u[1], w1);
+        u[2] = cmul(u[2], ld(2 * t));
     } else if constexpr (R == 4) {
         const float2 w2 = ld(2 * t);
         u[1] = cmul(u[1], w1);
@@ -150,15 +169,16 @@ struct ColSwz {
 // forms w^2..w^7 by products (see twiddle_reg).
 __host__ __device__ constexpr int tw_slots_upto(int N, int P)
 {
-    RadixList L = radix_list(N);
+    RadixList L = reg_radix_list(N);
+    const int V = reg_v(N), Q = N / reg_v(N);
     int slots = 0, ns = 1;
     for (int p = 0; p < P && p < L.n; ++p) {
-        if (p > 0) slots += (ns <= N / 8) ? 1 : 8 / L.r[p];
+        if (p > 0) slots += (Q % ns == 0) ? 1 : V / L.r[p];
         ns *= L.r[p];
     }
     return slots;
 }
-__host__ __device__ constexpr int tw_slots(int N) { return tw_slots_upto(N, radix_list(N).n); }
+__host__ __device__ constexpr int tw_slots(int N) { return tw_slots_upto(N, reg_radix_list(N).n); }
 
 template <int N>
 struct RegTw {
@@ -167,18 +187,19 @@ struct RegTw {
     template <int P, int NS>
     __device__ __forceinline__ void load_pass(const float2 *__restrict__ tw, int l)
     {
-        constexpr RadixList L = radix_list(N);
+        constexpr RadixList L = reg_radix_list(N);
         if constexpr (P < L.n) {
             constexpr int R = L.r[P];
-            constexpr int Q = N / 8;
+            constexpr int V = reg_v(N);
+            constexpr int Q = N / V;
             if constexpr (P > 0) {
                 constexpr int off = tw_slots_upto(N, P);
                 constexpr int STEP = N / (NS * R);
-                if constexpr (NS <= Q) {
-                    w[off] = __ldg(tw + (l & (NS - 1)) * STEP);
+                if constexpr (Q % NS == 0) {
+                    w[off] = __ldg(tw + (l % NS) * STEP);
                 } else {
 #pragma unroll
-                    for (int i = 0; i < 8 / R; ++i) w[off + i] = __ldg(tw + ((l + i * Q) & (NS - 1)) * STEP);
+                    for (int i = 0; i < V / R; ++i) w[off + i] = __ldg(tw + ((l + i * Q) % NS) * STEP);
                 }
             }
             load_pass<P + 1, NS * R>(tw, l);
@@ -198,6 +219,9 @@ __device__ __forceinline__ void twiddle_reg(float2 *u, float2 w1)
     if (S > 0) w1.y = -w1.y;
     if constexpr (R == 2) {
         u[1] = cmul(u[1], w1);
+    } else if constexpr (R == 3) {
+        u[1] = cmul(u[1], w1);
+        u[2] = cmul(u[2], cmul(w1, w1));
     } else if constexpr (R == 4) {
         const float2 w2 = cmul(w1, w1);
         u[1] = cmul(u[1], w1);
@@ -217,26 +241,27 @@ __device__ __forceinline__ void twiddle_reg(float2 *u, float2 w1)
 }
 
 template <int N, class LAYOUT, int S, int P, int NS>
-__device__ __forceinline__ void reg_passes_1buf_rt(float2 (&v)[8], float2 *buf, int b, int l,
+__device__ __forceinline__ void reg_passes_1buf_rt(float2 (&v)[reg_v(N)], float2 *buf, int b, int l,
                                                    const RegTw<N> &tw)
 {
-    constexpr RadixList L = radix_list(N);
+    constexpr RadixList L = reg_radix_list(N);
     if constexpr (P < L.n) {
         constexpr int R = L.r[P];
-        constexpr int BPT = 8 / R;
-        constexpr int Q = N / 8;
+        constexpr int V = reg_v(N);
+        constexpr int BPT = V / R;
+        constexpr int Q = N / V;
         int kk[BPT];
 #pragma unroll
         for (int i = 0; i < BPT; ++i) {
             const int j = l + i * Q;
-            const int k = j & (NS - 1);
+            const int k = j % NS;
             kk[i] = k;
             float2 u[R];
 #pragma unroll
             for (int q = 0; q < R; ++q) u[q] = v[i + q * BPT];
             if constexpr (NS > 1) {
                 constexpr int off = tw_slots_upto(N, P);
-                twiddle_reg<R, S>(u, tw.w[off + (NS <= Q ? 0 : i)]);
+                twiddle_reg<R, S>(u, tw.w[off + (Q % NS == 0 ? 0 : i)]);
             }
             dftR<R, S>(u);
 #pragma unroll
@@ -253,7 +278,7 @@ __device__ __forceinline__ void reg_passes_1buf_rt(float2 (&v)[8], float2 *buf, 
             }
             __syncthreads();
 #pragma unroll
-            for (int m = 0; m < 8; ++m) v[m] = buf[LAYOUT::at(b, l + m * Q)];
+            for (int m = 0; m < V; ++m) v[m] = buf[LAYOUT::at(b, l + m * Q)];
             reg_passes_1buf_rt<N, LAYOUT, S, P + 1, NS * R>(v, buf, b, l, tw);
         }
     }
@@ -261,27 +286,29 @@ __device__ __forceinline__ void reg_passes_1buf_rt(float2 (&v)[8], float2 *buf, 
 
 // As reg_fft_1buf, with the twiddles already in registers.
 template <int N, class LAYOUT, int S>
-__device__ __forceinline__ void reg_fft_1buf(float2 (&v)[8], float2 *buf, int b, int l, const RegTw<N> &tw)
+__device__ __forceinline__ void reg_fft_1buf(float2 (&v)[reg_v(N)], float2 *buf, int b, int l,
+                                             const RegTw<N> &tw)
 {
-    static_assert(is_pow2(N) && N >= 16, "pipelined FFT needs a power-of-two length >= 16");
+    static_assert((is_pow2(N) && N >= 16) || is_3pow2(N), "pipelined FFT length: 2^k >= 16 or 3*2^k >= 48");
     reg_passes_1buf_rt<N, LAYOUT, S, 0, 1>(v, buf, b, l, tw);
 }
 
 template <int N, class LAYOUT, int S, int P, int NS, bool SMEM_TW>
-__device__ __forceinline__ void reg_passes_1buf(float2 (&v)[8], float2 *buf, int b, int l,
+__device__ __forceinline__ void reg_passes_1buf(float2 (&v)[reg_v(N)], float2 *buf, int b, int l,
                                                 const float2 *__restrict__ tw)
 {
-    constexpr RadixList L = radix_list(N);
+    constexpr RadixList L = reg_radix_list(N);
     if constexpr (P < L.n) {
         constexpr int R = L.r[P];
-        constexpr int BPT = 8 / R;
-        constexpr int Q = N / 8;
+        constexpr int V = reg_v(N);
+        constexpr int BPT = V / R;
+        constexpr int Q = N / V;
         constexpr int STEP = N / (NS * R);
         int kk[BPT];
 #pragma unroll
         for (int i = 0; i < BPT; ++i) {
             const int j = l + i * Q;
-            const int k = j & (NS - 1);
+            const int k = j % NS;
             kk[i] = k;
             float2 u[R];
 #pragma unroll
@@ -302,21 +329,18 @@ __device__ __forceinline__ void reg_passes_1buf(float2 (&v)[8], float2 *buf, int
             }
             __syncthreads();
 #pragma unroll
-            for (int m = 0; m < 8; ++m) v[m] = buf[LAYOUT::at(b, l + m * Q)];
+            for (int m = 0; m < V; ++m) v[m] = buf[LAYOUT::at(b, l + m * Q)];
             reg_passes_1buf<N, LAYOUT, S, P + 1, NS * R, SMEM_TW>(v, buf, b, l, tw);
         }
     }
 }
 
-// Transform of the sequence in v through one exchange buffer.  Starts every
-// exchange with a barrier (so buf may still be read when it is called) and
-// leaves buf in use: callers synchronise before overwriting it.
 // tw: the length-N twiddle table, in global memory or (SMEM_TW) shared memory.
 template <int N, class LAYOUT, int S, bool SMEM_TW = false>
-__device__ __forceinline__ void reg_fft_1buf(float2 (&v)[8], float2 *buf, int b, int l,
+__device__ __forceinline__ void reg_fft_1buf(float2 (&v)[reg_v(N)], float2 *buf, int b, int l,
                                              const float2 *__restrict__ tw)
 {
-    static_assert(is_pow2(N) && N >= 16, "pipelined FFT needs a power-of-two length >= 16");
+    static_assert((is_pow2(N) && N >= 16) || is_3pow2(N), "pipelined FFT length: 2^k >= 16 or 3*2^k >= 48");
     reg_passes_1buf<N, LAYOUT, S, 0, 1, SMEM_TW>(v, buf, b, l, tw);
 }
 

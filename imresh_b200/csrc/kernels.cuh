@@ -53,14 +53,19 @@ __device__ __forceinline__ WorkItem item_at(const WorkList *L, int i)
 // T threads.  N = 0 selects the runtime-length FFT.
 // N < 0: Bluestein on the power-of-two length M = -N (one row per CTA;
 // column tiles of 8192/M columns).
-__host__ __device__ constexpr int row_nb(int N) { return N == 0 ? 0 : (N < 0 ? 1 : (N <= 2048 ? 2048 / N : 1)); }
+__host__ __device__ constexpr int row_nb(int N)
+{
+    return N == 0 ? 0 : (N < 0 ? 1 : (N % 3 == 0 ? (N <= 3072 ? 3072 / N : 1) : (N <= 2048 ? 2048 / N : 1)));
+}
 __host__ __device__ constexpr int row_threads(int N)
 {
     return N == 0 ? kRowThreads : (N < 0 ? (-N / 8 < 64 ? 64 : -N / 8) : 256);
 }
 __host__ __device__ constexpr int col_nb(int N)
 {
-    return N == 0 ? 0 : (N < 0 ? (8192 / -N > 8 ? 8 : (8192 / -N < 1 ? 1 : 8192 / -N)) : (N <= 2048 ? 8 : 4));
+    return N == 0 ? 0
+                  : (N < 0 ? (8192 / -N > 8 ? 8 : (8192 / -N < 1 ? 1 : 8192 / -N))
+                           : (N % 3 == 0 ? (N <= 384 ? 16 : (6144 / N < 2 ? 2 : 6144 / N)) : (N <= 2048 ? 8 : 4)));
 }
 __host__ __device__ constexpr int col_len(int N) { return N < 0 ? -N : N; }
 __host__ __device__ constexpr int col_threads(int N)
@@ -558,10 +563,15 @@ static __global__ void __launch_bounds__(256) k_vector_max(const float *d, long 
 // ============================================================================
 namespace imr {
 
-__host__ __device__ constexpr int rrow_nb(int N) { return N <= 2048 ? 2048 / N : 1; }
-__host__ __device__ constexpr int rrow_threads(int N) { return rrow_nb(N) * N / 8; }
-__host__ __device__ constexpr int rcol_nb(int N) { return N <= 1024 ? (8192 / N < 16 ? 8192 / N : 16) : (N == 2048 ? 4 : 2); }
-__host__ __device__ constexpr int rcol_threads(int N) { return rcol_nb(N) * N / 8; }
+// power-of-two lengths (8 values per thread); 3 * 2^k lengths (12 values per
+// thread) share their tile shapes with the per-tile kernels (row_nb, col_nb)
+__host__ __device__ constexpr int rrow_nb(int N) { return N % 3 == 0 ? row_nb(N) : (N <= 2048 ? 2048 / N : 1); }
+__host__ __device__ constexpr int rrow_threads(int N) { return rrow_nb(N) * N / reg_v(N); }
+__host__ __device__ constexpr int rcol_nb(int N)
+{
+    return N % 3 == 0 ? col_nb(N) : (N <= 1024 ? (8192 / N < 16 ? 8192 / N : 16) : (N == 2048 ? 4 : 2));
+}
+__host__ __device__ constexpr int rcol_threads(int N) { return rcol_nb(N) * N / reg_v(N); }
 __host__ __device__ constexpr int rrow_smem(int N) { return reg_smem_bytes(N, rrow_nb(N)); }
 __host__ __device__ constexpr int rcol_smem(int N) { return reg_smem_bytes(N, rcol_nb(N)); }
 
@@ -823,7 +833,7 @@ template <bool FIRST, int N>
 __global__ void __launch_bounds__(rrow_threads(N)) k_row_hio_p(const JobDev *jobs, const WorkList *L)
 {
     extern __shared__ __align__(128) unsigned char sbuf[];
-    constexpr int NB = rrow_nb(N), Q = N / 8;
+    constexpr int NB = rrow_nb(N), V = reg_v(N), Q = N / V;
     constexpr int XB = NB * N * 8;
     constexpr int STAGE = prow_stage_bytes<FIRST, N>();
     uint64_t *bars = reinterpret_cast<uint64_t *>(sbuf);
@@ -885,15 +895,15 @@ __global__ void __launch_bounds__(rrow_threads(N)) k_row_hio_p(const JobDev *job
         const int y = wi.tile * J.rpc + b;
         const bool ok = b < J.rpc && y < J.H;
         const size_t base = (size_t)y * N;
-        float2 v[8];
+        float2 v[V];
 #pragma unroll
-        for (int m = 0; m < 8; ++m) v[m] = sX[b * N + l + m * Q];
+        for (int m = 0; m < V; ++m) v[m] = sX[b * N + l + m * Q];
         reg_fft_1buf<N, RowSwz<N, NB>, +1>(v, sX, b, l, rtw);
         const float beta = J.beta;
         const float thr = st->thr;
         const bool init_gprev = FIRST && st->hio_cycle == 0;
 #pragma unroll
-        for (int m = 0; m < 8; ++m) {
+        for (int m = 0; m < V; ++m) {
             const int e = b * N + l + m * Q;
             const float2 gp1 = v[m];
             uint8_t msk;
@@ -915,7 +925,7 @@ __global__ void __launch_bounds__(rrow_threads(N)) k_row_hio_p(const JobDev *job
         reg_fft_1buf<N, RowSwz<N, NB>, -1>(v, sX, b, l, rtw);
         if (ok) {
 #pragma unroll
-            for (int m = 0; m < 8; ++m) J.X[base + l + m * Q] = v[m];
+            for (int m = 0; m < V; ++m) J.X[base + l + m * Q] = v[m];
         }
         fence_proxy_async_smem();
         __syncthreads();   // stage s is free for the copy issued next iteration
@@ -925,7 +935,8 @@ __global__ void __launch_bounds__(rrow_threads(N)) k_row_hio_p(const JobDev *job
 
 // ---- columns ------------------------------------------------------------------
 // stage: X tile [N][NB] complex | M tile [N][NB] float (when NB*4 >= 16)
-__host__ __device__ constexpr int pcol_box_rows(int N) { return N < 256 ? N : 256; }
+// rows per 2D TMA box: must divide N (boxes tile the column exactly)
+__host__ __device__ constexpr int pcol_box_rows(int N) { return N <= 256 ? N : (N % 3 == 0 ? 192 : 256); }
 __host__ __device__ constexpr bool pcol_tma_m(int N) { return rcol_nb(N) * 4 >= 16; }
 __host__ __device__ constexpr int pcol_threads(int N) { return rcol_threads(N); }
 template <int N>
@@ -941,7 +952,7 @@ template <int N>
 __global__ void __launch_bounds__(rcol_threads(N)) k_col_p(const JobDev *jobs, const WorkList *L)
 {
     extern __shared__ __align__(128) unsigned char sbuf[];
-    constexpr int NB = rcol_nb(N), Q = N / 8;
+    constexpr int NB = rcol_nb(N), V = reg_v(N), Q = N / V;
     constexpr int XB = NB * N * 8;
     constexpr int BR = pcol_box_rows(N);
     constexpr bool TM = pcol_tma_m(N);
@@ -1006,12 +1017,12 @@ __global__ void __launch_bounds__(rcol_threads(N)) k_col_p(const JobDev *jobs, c
         const int W = J.W;
         const int x = wi.tile * NB + b;
         const bool ok = x < W;
-        float2 v[8];
+        float2 v[V];
 #pragma unroll
-        for (int m = 0; m < 8; ++m) v[m] = sX[(l + m * Q) * NB + b];
+        for (int m = 0; m < V; ++m) v[m] = sX[(l + m * Q) * NB + b];
         reg_fft_1buf<N, ColSwz<N, NB>, -1, true>(v, sX, b, l, stw);
 #pragma unroll
-        for (int m = 0; m < 8; ++m) {
+        for (int m = 0; m < V; ++m) {
             float mod;
             if constexpr (TM) mod = reinterpret_cast<const float *>(stg + XB)[(l + m * Q) * NB + b];
             else mod = ok ? J.M[(size_t)(l + m * Q) * W + x] : 0.f;
@@ -1024,7 +1035,7 @@ __global__ void __launch_bounds__(rcol_threads(N)) k_col_p(const JobDev *jobs, c
         // the result goes back into the stage (tile layout) and leaves by TMA
         __syncthreads();
 #pragma unroll
-        for (int m = 0; m < 8; ++m) sX[(l + m * Q) * NB + b] = v[m];
+        for (int m = 0; m < V; ++m) sX[(l + m * Q) * NB + b] = v[m];
         fence_proxy_async_smem();
         __syncthreads();
         if (threadIdx.x == 0) {
