@@ -372,6 +372,13 @@ def run_ours(args, rank, world, local_rank):
     row_gbs = row_b / (ms_row * 1e-3) / 1e9
     col_gbs = col_b / (ms_col * 1e-3) / 1e9
     dom = ("row", row_b, ms_row, row_gbs) if ms_row >= ms_col else ("col", col_b, ms_col, col_gbs)
+    traffic = None
+    try:   # DRAM bytes per launch of the dominant kernel, from the committed ncu capture
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            tj = json.load(f)
+        traffic = tj.get("k_row_hio_p<0,2048>" if dom[0] == "row" else "k_col_p<2048>")
+    except Exception:
+        pass
     iter_gbs = (row_b + col_b) / ((ms_row + ms_col) * 1e-3) / 1e9
     launches = plan.launches() * args.steps
 
@@ -397,7 +404,8 @@ def run_ours(args, rank, world, local_rank):
                 "d2h_bytes_per_step": 4 * W * H,
                 "api": "imr_cuda_shrink_wrap (drop-in for cudaShrinkWrap), pinned host buffer"},
         "roofline": {"bound": "hbm", "achieved": dom[3], "peak": peak, "unit": "GB/s",
-                     "frac": dom[3] / peak, "traffic": None,
+                     "frac": dom[3] / peak, "traffic": traffic,
+                     "traffic_source": "profiles/traffic.json (ncu, cold cache, per launch)",
                      "kernel": f"{dom[0]} pass ({'k_row_hio' if dom[0] == 'row' else 'k_col'})",
                      "peak_source": peak_kind,
                      "algorithmic_bytes_per_launch": dom[1], "ms_per_launch": dom[2],
