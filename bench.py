@@ -432,7 +432,22 @@ def main():
     ap.add_argument("--serve", type=int, default=0, metavar="N",
                     help="only run the serving stream with N requests and print its JSON")
     ap.add_argument("--rate", type=float, default=20.0, help="serving arrival rate, requests/s")
+    ap.add_argument("--ncu-case", type=int, default=0, metavar="N",
+                    help="run one NxN reconstruction (1 cycle x 3 HIO) and exit: a small case for ncu")
     args = ap.parse_args()
+    if args.ncu_case:
+        import torch
+        import imresh_b200 as imr
+        from imresh_b200 import data
+        n = args.ncu_case
+        M, _ = data.make_modulus(data.BlobSpec(n, n, 60, 0.15 * n, (2.0, 2.0), (0.5, 1.0), None), 0)
+        plan = imr.Plan(n, n, imr.Params(1, imr.FLT_MIN, 0.9, 0.04, 0.2, 3.0, 0.01, 3))
+        d_m = torch.from_numpy(M).cuda()
+        d_o = torch.empty_like(d_m)
+        plan.execute(d_m, d_o)
+        torch.cuda.synchronize()
+        print(json.dumps({"ncu_case": n, "checksum": float(d_o.abs().sum())}))
+        return
     if args.serve:
         import torch
         torch.cuda.set_device(0)
