@@ -215,6 +215,23 @@ def run_served(n_req: int, rate_hz: float, seed: int = 4, max_side: int = 2048):
             "steps": info["steps"], "launches": info["launches"]}
 
 
+def max_over_ranks(values, dist=None, device=None):
+    """Element-wise max of a list of floats over all ranks (timings of the
+    slowest replica); identity without a process group."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.tolist()]
+
+
+def aggregate_throughput(steps: int, world: int, total_ms_max: float) -> float:
+    """Whole-job reconstructions per second: every rank runs `steps`
+    independent reconstructions; the job takes as long as the slowest rank."""
+    return steps * world / (total_ms_max / 1e3)
+
+
 def make_input():
     from imresh_b200 import data
     M, _ = data.make_modulus(data.cfg1_spec(), seed=1)
@@ -358,17 +375,13 @@ def run_ours(args, rank, world, local_rank):
         raise RuntimeError("non-finite reconstruction")
 
     e2e_total = float(sum(e2e_ms))
-    if dist is not None:
-        t = torch.tensor([total_ms, e2e_total, ms_row, ms_col], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms, e2e_total, ms_row, ms_col = [float(x) for x in t.tolist()]
+    total_ms, e2e_total, ms_row, ms_col = max_over_ranks([total_ms, e2e_total, ms_row, ms_col], dist, dev)
 
     if rank != 0:
         return
     peak, peak_kind = _peaks()
-    n_rec = args.steps * world
-    value = n_rec / (total_ms / 1e3)
-    e2e_value = n_rec / (e2e_total / 1e3)
+    value = aggregate_throughput(args.steps, world, total_ms)
+    e2e_value = aggregate_throughput(args.steps, world, e2e_total)
     row_gbs = row_b / (ms_row * 1e-3) / 1e9
     col_gbs = col_b / (ms_col * 1e-3) / 1e9
     dom = ("row", row_b, ms_row, row_gbs) if ms_row >= ms_col else ("col", col_b, ms_col, col_gbs)
