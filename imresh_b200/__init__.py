@@ -360,3 +360,106 @@ def diffraction_intensity(obj: np.ndarray) -> np.ndarray:
     H, W = a.shape
     _check(L.imr_diffraction_intensity(a.ctypes.data, W, H, _stream(None)), "imr_diffraction_intensity")
     return a
+
+
+# ------------------------------------------------------------------ fixed-support HIO
+HIO_SEED = 2623091912   # srand() seed of libs::addRandomPhase (hybridInputOutput.cpp:160)
+MASK_F32, MASK_U8 = 0, 1
+
+
+def _hio_sigs(L):
+    vp, u, f, i = C.c_void_p, C.c_uint, C.c_float, C.c_int
+    L.imr_hybrid_input_output.argtypes = [vp, vp, u, u, u, f, f, vp]
+    L.imr_hio_plan_create.argtypes = [C.POINTER(vp), u, u, u, f, f]
+    L.imr_hio_plan_execute.argtypes = [vp, vp, vp, vp, u, vp]
+    L.imr_hio_plan_execute_host.argtypes = [vp, vp, vp, vp, u, vp]
+    L.imr_hio_plan_stats.argtypes = [vp, vp, C.POINTER(i), C.POINTER(f), vp, i]
+    L.imr_hio_plan_destroy.argtypes = [vp]
+    L.imr_calculate_hio_error.argtypes = [vp, vp, i, C.c_size_t, i, C.POINTER(f), C.POINTER(f),
+                                          C.POINTER(f), vp]
+    L.imr_rand_field.argtypes = [vp, C.c_size_t, u, vp]
+
+
+def rand_field(d_out, n: int, seed: int = HIO_SEED, stream=None):
+    """Device complex64 ((float)rand()/RAND_MAX, 0) after srand(seed)."""
+    L = lib()
+    _hio_sigs(L)
+    _check(L.imr_rand_field(_ptr(d_out), n, seed, _stream(stream)), "imr_rand_field")
+
+
+def hybrid_input_output(io: np.ndarray, mask: np.ndarray, n_cycles: int = 0,
+                        target_error: float = 1e-6, beta: float = 0.9, stream=0) -> int:
+    """libs::hybridInputOutput: ``io`` (float32 [H][W], host) holds the Fourier
+    modulus on entry and Re(g') on return; ``mask`` (uint8 [H][W]) is 1 outside
+    the support.  Defaults as the reference's (hybridInputOutput.hpp:81-90).
+    Returns 0 on success, else an imr_status code."""
+    if io.dtype != np.float32 or not io.flags.c_contiguous or io.ndim != 2:
+        raise ValueError("io must be a C-contiguous float32 [H][W] array")
+    m = np.ascontiguousarray(mask, dtype=np.uint8)
+    if m.shape != io.shape:
+        raise ValueError("mask must have the shape of io")
+    L = lib()
+    _hio_sigs(L)
+    H, W = io.shape
+    return L.imr_hybrid_input_output(io.ctypes.data, m.ctypes.data, W, H, n_cycles, target_error,
+                                     beta, _stream(stream) if stream else 0)
+
+
+class HioPlan:
+    """Reusable fixed-support HIO plan (random initial phase) for one size."""
+
+    def __init__(self, width: int, height: int, n_cycles: int = 0, target_error: float = 1e-6,
+                 beta: float = 0.9):
+        L = lib()
+        _hio_sigs(L)
+        self.width, self.height = width, height
+        h = C.c_void_p()
+        _check(L.imr_hio_plan_create(C.byref(h), width, height, n_cycles, target_error, beta),
+               "imr_hio_plan_create")
+        self._h = h
+
+    def execute(self, d_modulus, d_mask, d_out, seed: int = HIO_SEED, stream=None):
+        _check(lib().imr_hio_plan_execute(self._h, _ptr(d_modulus), _ptr(d_mask), _ptr(d_out), seed,
+                                          _stream(stream)), "imr_hio_plan_execute")
+
+    def execute_host(self, modulus: np.ndarray, mask: np.ndarray, out: np.ndarray | None = None,
+                     seed: int = HIO_SEED, stream=None):
+        m = np.ascontiguousarray(modulus, dtype=np.float32)
+        k = np.ascontiguousarray(mask, dtype=np.uint8)
+        if out is None:
+            out = np.empty_like(m)
+        _check(lib().imr_hio_plan_execute_host(self._h, _ptr(m), _ptr(k), _ptr(out), seed,
+                                               _stream(stream)), "imr_hio_plan_execute_host")
+        return out
+
+    def stats(self, cap: int = 4096, stream=None):
+        """(iterations, last tested error, per-iteration errors)."""
+        n, e = C.c_int(), C.c_float()
+        errs = np.zeros(cap, np.float32)
+        _check(lib().imr_hio_plan_stats(self._h, _stream(stream), C.byref(n), C.byref(e),
+                                        errs.ctypes.data, cap), "imr_hio_plan_stats")
+        return n.value, e.value, errs[:min(n.value + 1, cap)]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().imr_hio_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def calculate_hio_error(d_data, d_mask, n: int, invert_mask: bool = False, stream=None):
+    """cudaCalculateHioError over device buffers: (total, count, error).  The
+    mask is float32 or uint8 (a torch tensor's dtype decides)."""
+    L = lib()
+    _hio_sigs(L)
+    kind = MASK_U8 if str(getattr(d_mask, "dtype", "")).endswith("uint8") else MASK_F32
+    t, c, e = C.c_float(), C.c_float(), C.c_float()
+    _check(L.imr_calculate_hio_error(_ptr(d_data), _ptr(d_mask), kind, n, int(invert_mask),
+                                     C.byref(t), C.byref(c), C.byref(e), _stream(stream)),
+           "imr_calculate_hio_error")
+    return t.value, c.value, e.value

@@ -5,7 +5,10 @@
 //                                               worker thread, write-out
 //                                               callbacks on a second thread
 //   imresh::io::writeOutFuncs::justFree       -> delete[]
+//   imresh::libs::diffractionIntensity        -> imr_diffraction_intensity
+//   imresh::libs::hybridInputOutput           -> imr_hybrid_input_output
 #include <cuda_runtime.h>
+#include <limits.h>
 #include <stdio.h>
 
 #include <condition_variable>
@@ -20,6 +23,7 @@
 #include "imresh/algorithms/cuda/cudaShrinkWrap.hpp"
 #include "imresh/io/taskQueue.hpp"
 #include "imresh/io/writeOutFuncs/writeOutFuncs.hpp"
+#include "imresh/libs/hybridInputOutput.hpp"
 
 namespace imresh
 {
@@ -50,6 +54,19 @@ namespace libs
         int rc = imr_diffraction_intensity(rpIoData, rImageWidth, rImageHeight, (void *)rStream);
         if (rc != IMR_SUCCESS)
             fprintf(stderr, "imresh_b200 diffractionIntensity: %s\n", imr_status_string(rc));
+    }
+
+    // hybridInputOutput (src/imresh/libs/hybridInputOutput.hpp:81-90): rSize =
+    // {rows, columns} as the reference's FFTW plan takes it; 1 for a wrong
+    // dimension count or a NULL buffer, as the reference (cpp:199-206).
+    int hybridInputOutput(float *const rIoData, uint8_t const *const rMask,
+                          std::vector<unsigned int> const rSize, unsigned int rnCycles,
+                          float rTargetError, float rBeta, unsigned int)
+    {
+        if (rSize.size() != 2 || rIoData == NULL || rMask == NULL) return 1;
+        return imr_hybrid_input_output(rIoData, rMask, rSize[1], rSize[0],
+                                       rnCycles == UINT_MAX ? 0u : rnCycles, rTargetError, rBeta,
+                                       nullptr);
     }
 } // namespace libs
 

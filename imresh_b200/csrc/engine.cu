@@ -215,23 +215,32 @@ int gaussian_weights(double sigma, float *w, int cap)
 template <int N>
 static RowKernels row_set()
 {
-    if constexpr (N >= 16 && is_pow2(N))
-        return RowKernels{k_row_hio_r<true, N>, k_row_hio_r<false, N>, k_row_finish_r<N>,
-                          k_fft_rows_r<-1, N>, k_fft_rows_r<+1, N>, rrow_nb(N), rrow_threads(N),
-                          rrow_smem(N), k_row_hio_p<true, N>, k_row_hio_p<false, N>,
-                          prow_smem<true, N>(), prow_smem<false, N>(), 0};
-    else if constexpr (N >= 8 && is_pow2(N))
-        return RowKernels{k_row_hio_r<true, N>, k_row_hio_r<false, N>, k_row_finish_r<N>,
-                          k_fft_rows_r<-1, N>, k_fft_rows_r<+1, N>, rrow_nb(N), rrow_threads(N),
-                          rrow_smem(N), nullptr, nullptr, 0, 0, 0};
-    else if constexpr (is_3pow2(N))   // per-tile kernels + pipelined 12-value register passes
-        return RowKernels{k_row_hio<true, N>, k_row_hio<false, N>, k_row_finish<N>, k_fft_rows<-1, N>,
-                          k_fft_rows<+1, N>, row_nb(N), row_threads(N), 0, k_row_hio_p<true, N>,
-                          k_row_hio_p<false, N>, prow_smem<true, N>(), prow_smem<false, N>(), 0};
-    else
-        return RowKernels{k_row_hio<true, N>, k_row_hio<false, N>, k_row_finish<N>, k_fft_rows<-1, N>,
-                          k_fft_rows<+1, N>, row_nb(N), row_threads(N), 0, nullptr, nullptr, 0, 0,
-                          N < 0 ? -N : 0};
+    RowKernels k{};
+    if constexpr (N >= 16 && is_pow2(N)) {
+        k = RowKernels{k_row_hio_r<true, N>, k_row_hio_r<false, N>, k_row_finish_r<N>,
+                       k_fft_rows_r<-1, N>, k_fft_rows_r<+1, N>, rrow_nb(N), rrow_threads(N),
+                       rrow_smem(N), k_row_hio_p<true, N>, k_row_hio_p<false, N>,
+                       prow_smem<true, N>(), prow_smem<false, N>(), 0};
+        k.hio_fix = k_row_hio_r<false, N, true>;
+        k.p_hio_fix = k_row_hio_p<false, N, true>;
+    } else if constexpr (N >= 8 && is_pow2(N)) {
+        k = RowKernels{k_row_hio_r<true, N>, k_row_hio_r<false, N>, k_row_finish_r<N>,
+                       k_fft_rows_r<-1, N>, k_fft_rows_r<+1, N>, rrow_nb(N), rrow_threads(N),
+                       rrow_smem(N), nullptr, nullptr, 0, 0, 0};
+        k.hio_fix = k_row_hio_r<false, N, true>;
+    } else if constexpr (is_3pow2(N)) {   // per-tile kernels + pipelined 12-value register passes
+        k = RowKernels{k_row_hio<true, N>, k_row_hio<false, N>, k_row_finish<N>, k_fft_rows<-1, N>,
+                       k_fft_rows<+1, N>, row_nb(N), row_threads(N), 0, k_row_hio_p<true, N>,
+                       k_row_hio_p<false, N>, prow_smem<true, N>(), prow_smem<false, N>(), 0};
+        k.hio_fix = k_row_hio<false, N, true>;
+        k.p_hio_fix = k_row_hio_p<false, N, true>;
+    } else {
+        k = RowKernels{k_row_hio<true, N>, k_row_hio<false, N>, k_row_finish<N>, k_fft_rows<-1, N>,
+                       k_fft_rows<+1, N>, row_nb(N), row_threads(N), 0, nullptr, nullptr, 0, 0,
+                       N < 0 ? -N : 0};
+        k.hio_fix = k_row_hio<false, N, true>;
+    }
+    return k;
 }
 template <int N>
 static ColKernels col_set()
@@ -382,6 +391,8 @@ int ensure_kernel_attributes()
         if (e == cudaSuccess) e = allow_smem(c.fft_inv);
         if (e == cudaSuccess && r.p_hio) e = allow_smem(r.p_hio);
         if (e == cudaSuccess && r.p_hio_first) e = allow_smem(r.p_hio_first);
+        if (e == cudaSuccess) e = allow_smem(r.hio_fix);
+        if (e == cudaSuccess && r.p_hio_fix) e = allow_smem(r.p_hio_fix);
         if (e == cudaSuccess && c.p_col) e = allow_smem(c.p_col);
     }
     if (e == cudaSuccess) e = allow_smem(k_hblur);
@@ -421,6 +432,33 @@ int build_weight_table(const imr_params &p, std::vector<float> &w, std::vector<i
         if (K > kMaxTaps) return IMR_ERR_INVALID_VALUE;
         taps[c] = K;
         sigma = fmaxf(1.5f, (1.0f - p.sigmaChange) * sigma);
+    }
+    return IMR_SUCCESS;
+}
+
+// Unnormalised 2D transform passes over a [H][W] complex array with the
+// plain FFT kernels: axes bit 1 = rows, bit 2 = columns; sign -1 runs rows
+// then columns, +1 columns then rows.
+int fft_passes(float2 *d, int W, int H, int sign, int axes, const FftPlanDev &pr, const FftPlanDev &pc,
+               cudaStream_t s)
+{
+    const RowKernels rk = row_kernels(W);
+    const ColKernels ck = col_kernels(H);
+    const int rpc = rk.nb, cpc = ck.nb;
+    const int nrt = (H + rpc - 1) / rpc, nct = (W + cpc - 1) / cpc;
+    const size_t sr = rk.smem ? (size_t)rk.smem : ((size_t)rpc * W + rk.bs_m) * 8;
+    const size_t sc = ck.smem ? (size_t)ck.smem : ((size_t)H + ck.bs_m) * cpc * 8;
+    if (sign < 0) {
+        if (axes & 1) rk.fft_fwd<<<nrt, rk.threads, sr, s>>>(d, pr, H, rpc);
+        if (axes & 2) ck.fft_fwd<<<nct, ck.threads, sc, s>>>(d, pc, W, cpc);
+    } else {
+        if (axes & 2) ck.fft_inv<<<nct, ck.threads, sc, s>>>(d, pc, W, cpc);
+        if (axes & 1) rk.fft_inv<<<nrt, rk.threads, sr, s>>>(d, pr, H, rpc);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error("fft launch", e);
+        return IMR_ERR_CUDA;
     }
     return IMR_SUCCESS;
 }
@@ -586,7 +624,8 @@ int job_upload(const JobDev &J, const JobShape &S, char *a, JobDev *dj, cudaStre
     CK(cudaMemcpyAsync(a + S.oT, S.taps.data(), S.taps.size() * 4, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(dj, &J, sizeof(JobDev), cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(a + S.oMask, 0, N, s));
-    CK(cudaMemsetAsync(a + S.oErr, 0, (size_t)(J.n_cycles + 1) * 4, s));
+    const size_t n_err = J.mode == kModeHio ? (size_t)J.n_err : (size_t)J.n_cycles + 1;   // allocated length
+    CK(cudaMemsetAsync(a + S.oErr, 0, n_err * 4, s));
     return IMR_SUCCESS;
 }
 }  // namespace imr
@@ -861,23 +900,7 @@ int imr_fft2d(void *d_data, unsigned W, unsigned H, int sign, void *stream)
     if (rc) return rc;
     FftPlanDev pr, pc;
     if ((rc = make_fft_plan((int)W, pr)) || (rc = make_fft_plan((int)H, pc))) return rc;
-    const RowKernels rk = row_kernels((int)W);
-    const ColKernels ck = col_kernels((int)H);
-    const int rpc = rk.nb, cpc = ck.nb;
-    cudaStream_t s = (cudaStream_t)stream;
-    float2 *d = (float2 *)d_data;
-    const int nrt = ((int)H + rpc - 1) / rpc, nct = ((int)W + cpc - 1) / cpc;
-    const size_t sr = rk.smem ? (size_t)rk.smem : ((size_t)rpc * W + rk.bs_m) * 8;
-    const size_t sc = ck.smem ? (size_t)ck.smem : ((size_t)H + ck.bs_m) * cpc * 8;
-    if (sign < 0) {
-        rk.fft_fwd<<<nrt, rk.threads, sr, s>>>(d, pr, (int)H, rpc);
-        ck.fft_fwd<<<nct, ck.threads, sc, s>>>(d, pc, (int)W, cpc);
-    } else {
-        ck.fft_inv<<<nct, ck.threads, sc, s>>>(d, pc, (int)W, cpc);
-        rk.fft_inv<<<nrt, rk.threads, sr, s>>>(d, pr, (int)H, rpc);
-    }
-    CK(cudaGetLastError());
-    return IMR_SUCCESS;
+    return fft_passes((float2 *)d_data, (int)W, (int)H, sign, 3, pr, pc, (cudaStream_t)stream);
 }
 
 int imr_gaussian_blur(float *d_data, float *d_tmp, unsigned W, unsigned H, double sigma, int axes,

@@ -14,6 +14,9 @@
 //   hb   float32   [H][W]  |g'| blurred along rows
 //   vb   float32   [H][W]  |g'| blurred along rows and columns
 //   out  float32   [H][W]  Re(g') -- the result
+// The same layout serves the fixed-support HIO of libs::hybridInputOutput
+// (mode 1): the caller's mask, a random initial phase, no blur, an error and
+// stop test after every iteration.
 // All per-cycle control (sigma weights, threshold, error, stop test) stays on
 // the device, so a reconstruction runs without host synchronisation.
 #pragma once
@@ -36,20 +39,25 @@ constexpr int kVbThreads = 256;
 
 struct JobState {
     int cycle;          // cycle whose mask is being built by finish/vblur
+                        // (mode 1: the iteration whose g' the next row pass makes)
     int hio_cycle;      // cycle whose HIO block is running
     int stop;           // 1: finished; every later launch returns at once
-    int cycles_done;    // HIO blocks completed and error-tested
+    int cycles_done;    // HIO blocks completed and error-tested (mode 1: iterations)
     float thr;          // support threshold of the running cycle
     unsigned max_bits;  // max of the blurred |g'| (float bits, values >= 0)
-    unsigned counter;   // last-block detection in the vertical blur pass
+    unsigned counter;   // last-block detection (vertical blur pass; mode 1: row pass)
     float last_error;
     int err;            // nonzero: a device-side wait gave up (see tma.cuh)
 };
+
+constexpr int kModeShrinkWrap = 0;
+constexpr int kModeHio = 1;   // fixed support, random initial phase
 
 struct alignas(64) JobDev {
     CUtensorMap tmX;    // X as W x H 8-byte elements, box (cpc, rows)
     CUtensorMap tmM;    // M as W x H floats, box (cpc, rows)
     int use_tma_cols;   // 1: column pass reads tiles through tmX / tmM
+    int mode;           // kModeShrinkWrap / kModeHio
     int W, H;
     float2 *X;
     float2 *G;
@@ -65,7 +73,8 @@ struct alignas(64) JobDev {
     const float *weights;   // [(n_cycles + 1) * kTapStride]
     const int *ntaps;       // [n_cycles + 1]
     double *err_part;       // [2 * n_row_tiles]  (sum mask*|g'|, sum mask)
-    float *errors;          // [n_cycles] error after each cycle
+    float *errors;          // [n_cycles] error after each cycle (mode 1: [n_err] per iteration)
+    int n_err;              // mode 1: length of errors
     JobState *st;
     int rpc;                // rows per row-pass CTA
     int cpc;                // columns per column-pass CTA

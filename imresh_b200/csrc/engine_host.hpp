@@ -36,6 +36,10 @@ struct RowKernels {
     void (*p_hio)(const JobDev *, const WorkList *);
     int p_smem_first, p_smem;
     int bs_m;      // Bluestein work length (0: direct transform)
+    // fixed-support HIO row passes (libs::hybridInputOutput): per-tile kernel
+    // and, where the length has one, the pipelined kernel (shared memory p_smem)
+    void (*hio_fix)(const JobDev *, const WorkList *);
+    void (*p_hio_fix)(const JobDev *, const WorkList *);
 };
 // Kernels and launch shape of the column passes for one column length.
 struct ColKernels {
@@ -55,6 +59,9 @@ struct ColKernels {
 };
 RowKernels row_kernels(int N);
 ColKernels col_kernels(int N);
+// Plain 2D transform passes (axes: 1 rows, 2 columns, 3 both).
+int fft_passes(float2 *d, int W, int H, int sign, int axes, const FftPlanDev &pr, const FftPlanDev &pc,
+               cudaStream_t s);
 // Persistent grid size for a pipelined kernel (CTAs per SM x SMs, <= items).
 int persistent_grid(const void *kernel, int threads, int smem, int items);
 // 2D tensor map over a row-major [H][W] array of `elem`-byte elements with a

@@ -133,6 +133,65 @@ __device__ __forceinline__ void block_sum2(double &a, double &b, double *scratch
     __syncthreads();
 }
 
+// Fixed-support HIO (libs::hybridInputOutput, src/imresh/libs/hybridInputOutput.cpp:237-292):
+// every row pass makes g'_k.  Each tile's sums (sum mask*|g'|, sum mask) are
+// stored per tile; the CTA that completes the job's last tile of the pass
+// forms E_k = sqrt(sum)/count (calculateHioError, cpp:67-103, summed in double
+// in a fixed order), applies the stop tests E_k < target (cpp:251-254) and
+// k == nCycles (cpp:255-256), and moves the job to iteration k + 1.
+template <int T>
+__device__ __forceinline__ void hio_tile_done(const JobDev &J, int tile, double tot, double cnt)
+{
+    __shared__ double red[2 * (T / 32 > 1 ? T / 32 : 1)];
+    __shared__ int s_last;
+    JobState *st = J.st;
+    block_sum2<T>(tot, cnt, red);
+    if (threadIdx.x == 0) {
+        J.err_part[2 * tile] = tot;
+        J.err_part[2 * tile + 1] = cnt;
+        __threadfence();
+        s_last = atomicAdd(&st->counter, 1u) == (unsigned)J.n_row_tiles - 1u;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    tot = 0.0;
+    cnt = 0.0;
+    const volatile double *ep = J.err_part;
+    for (int t = threadIdx.x; t < J.n_row_tiles; t += T) {
+        tot += ep[2 * t];
+        cnt += ep[2 * t + 1];
+    }
+    block_sum2<T>(tot, cnt, red);
+    if (threadIdx.x == 0) {
+        const int k = st->cycle;
+        int stop = k >= J.n_cycles;
+        if (J.target > 0.f || stop) {
+            const float E = (float)(sqrt(tot) / cnt);
+            st->last_error = E;
+            if (k < J.n_err) J.errors[k] = E;
+            if (J.target > 0.f && E < J.target) stop = 1;
+        }
+        st->cycles_done = k;
+        st->cycle = k + 1;
+        st->counter = 0u;
+        if (stop) st->stop = 1;
+        __threadfence();
+    }
+}
+
+// Per-element part of the fixed-support HIO row pass: error terms of g' and
+// out = Re(g') when this iteration is tested (or is the last).
+__device__ __forceinline__ void hio_track(const JobDev &J, size_t idx, float2 gp1, uint8_t m, double &tot,
+                                          double &cnt)
+{
+    if (m) {
+        tot += (double)m * (double)cnorm_ref(gp1);
+        cnt += (double)m;
+    }
+    J.out[idx] = gp1.x;
+}
+
 template <int NT>
 __device__ __forceinline__ float block_max(float v, float *scratch)
 {
@@ -229,7 +288,8 @@ __global__ void __launch_bounds__(col_threads(N)) k_col_init(const JobDev *jobs,
 // ---------------------------------------------------------------- column pass
 // Forward column FFT, G <- G * M/|G| (|G| = 0 -> 1; applyComplexModulus,
 // src/imresh/algorithms/cuda/cudaVectorElementwise.cu:168-195), inverse
-// column FFT.
+// column FFT.  Fixed-support HIO jobs divide without the |G| = 0 guard, as
+// libs::hybridInputOutput does (src/imresh/libs/hybridInputOutput.cpp:281-289).
 template <int N>
 __device__ __forceinline__ void b_col(const JobDev *jobs, const WorkItem wi)
 {
@@ -252,7 +312,7 @@ __device__ __forceinline__ void b_col(const JobDev *jobs, const WorkItem wi)
         const int y = i / nc, c = i - y * nc;
         const float2 g = sm[y * es + c];
         float nrm = cnorm_ref(g);
-        if (nrm == 0.f) nrm = 1.f;
+        if (nrm == 0.f && J.mode == kModeShrinkWrap) nrm = 1.f;
         const float f = __fdiv_rn(J.M[(size_t)y * W + x0 + c], nrm);
         sm[y * es + c] = make_float2(__fmul_rn(g.x, f), __fmul_rn(g.y, f));
     }
@@ -277,7 +337,11 @@ __global__ void __launch_bounds__(col_threads(N)) k_col(const JobDev *jobs, cons
 // FIRST: first iteration of a cycle -- builds the uint8 mask from the blurred
 // image (mask = blurred < threshold, cudaKernelCutOff, cudaVectorElementwise.cu:198-219)
 // and, on cycle 0, takes g_prev = g'_0 (cudaShrinkWrap.cu:304-309).
-template <bool FIRST, int N>
+// FIX: fixed-support HIO of libs::hybridInputOutput -- the caller's mask
+// (HIO where mask == 1, error weight = mask value, hybridInputOutput.cpp:262-269),
+// g_prev = g'_0 on iteration 0 (cpp:245-246), error terms and out = Re(g')
+// on every tested iteration, no update on the last one (hio_tile_done).
+template <bool FIRST, int N, bool FIX = false>
 __device__ __forceinline__ void b_row_hio(const JobDev *jobs, const WorkItem wi)
 {
     extern __shared__ float4 smem4[];
@@ -296,7 +360,11 @@ __device__ __forceinline__ void b_row_hio(const JobDev *jobs, const WorkItem wi)
     fft_rows<N, +1>(sm, nr, J.prow);
     const float beta = J.beta;
     const float thr = st->thr;
-    const bool init_gprev = FIRST && st->hio_cycle == 0;
+    const int k = FIX ? st->cycle : 0;
+    const bool init_gprev = FIX ? k == 0 : FIRST && st->hio_cycle == 0;
+    const bool fin = FIX && k >= J.n_cycles;
+    const bool track = FIX && (J.target > 0.f || fin);
+    double tot = 0.0, cnt = 0.0;
     for (int i = threadIdx.x; i < n; i += T) {
         const size_t idx = base + i;
         const float2 gp1 = sm[i];   // g'
@@ -307,9 +375,13 @@ __device__ __forceinline__ void b_row_hio(const JobDev *jobs, const WorkItem wi)
         } else {
             m = J.mask[idx];
         }
+        if (FIX) {
+            if (track) hio_track(J, idx, gp1, m, tot, cnt);
+            if (fin) continue;
+        }
         const float2 gp = init_gprev ? gp1 : J.G[idx];
         float2 g;
-        if (m || gp1.x < 0.f)
+        if ((FIX ? m == 1 : m != 0) || gp1.x < 0.f)
             g = make_float2(__fsub_rn(gp.x, __fmul_rn(beta, gp1.x)),
                             __fsub_rn(gp.y, __fmul_rn(beta, gp1.y)));
         else
@@ -317,14 +389,17 @@ __device__ __forceinline__ void b_row_hio(const JobDev *jobs, const WorkItem wi)
         J.G[idx] = g;
         sm[i] = g;
     }
-    __syncthreads();
-    fft_rows<N, -1>(sm, nr, J.prow);
-    for (int i = threadIdx.x; i < n; i += T) J.X[base + i] = sm[i];
+    if (!fin) {
+        __syncthreads();
+        fft_rows<N, -1>(sm, nr, J.prow);
+        for (int i = threadIdx.x; i < n; i += T) J.X[base + i] = sm[i];
+    }
+    if (FIX) hio_tile_done<T>(J, wi.tile, tot, cnt);
 }
-template <bool FIRST, int N>
+template <bool FIRST, int N, bool FIX = false>
 __global__ void __launch_bounds__(row_threads(N)) k_row_hio(const JobDev *jobs, const WorkList *L)
 {
-    IMR_ITEM_LOOP((b_row_hio<FIRST, N>(jobs, wi)));
+    IMR_ITEM_LOOP((b_row_hio<FIRST, N, FIX>(jobs, wi)));
 }
 
 // Once per cycle: inverse row FFT -> g'; out = Re(g') (CopyFromRealPart,
@@ -531,6 +606,120 @@ static __global__ void k_complex_norm(const float2 *src, float *dst, long n)
         dst[i] = cnorm_ref(src[i]);
 }
 
+// ---------------------------------------------------------------- random phase
+// The C library's rand() stream as libs::addRandomPhase draws it after
+// srand(2623091912) (src/imresh/libs/hybridInputOutput.cpp:160-167): glibc's
+// additive feedback generator, r[i] = r[i-31] + r[i-3] (mod 2^32) for i >= 34,
+// rand() number k = r[k + 344] >> 1.  Thread c makes the numbers
+// [c*kRandChunk, (c+1)*kRandChunk): its 31-word state (r[i-31..i-1]) starts
+// from the base state at i = 344 and jumps by B^c, B = A^kRandChunk the
+// recurrence's 31x31 step matrix over Z/2^32 raised to the chunk length,
+// composed from the table pow[j] = B^(2^j); then it runs the recurrence.
+// Element k of X becomes ((float)rand_k / RAND_MAX, 0) (cpp:163-167).
+constexpr int kRandLag = 31;
+constexpr int kRandChunk = 31 * 32;
+constexpr int kRandThreads = 128;
+struct RandBase {
+    uint32_t s[kRandLag];
+};
+static __global__ void __launch_bounds__(kRandThreads) k_rand_field(float2 *X, long n, RandBase base,
+                                                                    const uint32_t *pow, int n_pow)
+{
+    __shared__ uint32_t P[kRandLag * kRandLag];
+    const long c = (long)blockIdx.x * kRandThreads + threadIdx.x;
+    uint32_t s[kRandLag];
+#pragma unroll
+    for (int i = 0; i < kRandLag; ++i) s[i] = base.s[i];
+    for (int j = 0; j < n_pow; ++j) {
+        __syncthreads();
+        for (int i = threadIdx.x; i < kRandLag * kRandLag; i += kRandThreads)
+            P[i] = pow[(size_t)j * kRandLag * kRandLag + i];
+        __syncthreads();
+        if ((c >> j) & 1) {
+            uint32_t t[kRandLag];
+#pragma unroll
+            for (int i = 0; i < kRandLag; ++i) {
+                uint32_t a = 0;
+#pragma unroll
+                for (int m = 0; m < kRandLag; ++m) a += P[i * kRandLag + m] * s[m];
+                t[i] = a;
+            }
+#pragma unroll
+            for (int i = 0; i < kRandLag; ++i) s[i] = t[i];
+        }
+    }
+    const long k0 = c * kRandChunk;
+    if (k0 >= n) return;
+    const long kend = min(n, k0 + kRandChunk);
+    for (int o = 0; o < kRandChunk / kRandLag; ++o) {
+#pragma unroll
+        for (int q = 0; q < kRandLag; ++q) {
+            const uint32_t r = s[q] + s[(q + kRandLag - 3) % kRandLag];   // r[i-31] + r[i-3]
+            s[q] = r;
+            const long k = k0 + (long)o * kRandLag + q;
+            if (k < kend) X[k] = make_float2(__fdiv_rn((float)(int)(r >> 1), 2147483648.0f), 0.f);
+        }
+    }
+}
+
+// X = M * (cos phase, sin phase), phase = arg(X) of the transformed random
+// field (addRandomPhase, hybridInputOutput.cpp:170-180).  The reference's
+// unqualified cos/sin of a float resolve to the double functions, so the
+// products are formed in double and rounded to float, as there.
+static __global__ void k_random_phase(float2 *X, const float *M, long n)
+{
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const float2 z = X[i];
+        const float ph = atan2f(z.y, z.x);
+        double sn, cs;
+        sincos((double)ph, &sn, &cs);
+        const double m = (double)M[i];
+        X[i] = make_float2((float)(m * cs), (float)(m * sn));
+    }
+}
+
+// cudaCalculateHioError (src/imresh/algorithms/cuda/cudaVectorReduce.cu:284-403):
+// sums of w*|z| and of w, w = (mask != 0) xor invert.  Block sums in double;
+// the last block folds them in block order (deterministic) into res[0..1].
+template <class TM>
+static __global__ void __launch_bounds__(256) k_hio_error(const float2 *d, const TM *mask, long n, int invert,
+                                                          double *part, unsigned *counter, double *res)
+{
+    __shared__ double red[16];
+    __shared__ int s_last;
+    double tot = 0.0, cnt = 0.0;
+    for (long i = blockIdx.x * 256L + threadIdx.x; i < n; i += (long)gridDim.x * 256) {
+        const bool w = (mask[i] != TM(0)) != (invert != 0);
+        if (w) {
+            tot += (double)cnorm_ref(d[i]);
+            cnt += 1.0;
+        }
+    }
+    block_sum2<256>(tot, cnt, red);
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = tot;
+        part[2 * blockIdx.x + 1] = cnt;
+        __threadfence();
+        s_last = atomicAdd(counter, 1u) == gridDim.x - 1u;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    tot = 0.0;
+    cnt = 0.0;
+    const volatile double *vp = part;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += 256) {
+        tot += vp[2 * b];
+        cnt += vp[2 * b + 1];
+    }
+    block_sum2<256>(tot, cnt, red);
+    if (threadIdx.x == 0) {
+        res[0] = tot;
+        res[1] = cnt;
+        *counter = 0u;
+    }
+}
+
 // Global max of a float array (vectorMax; cudaVectorReduce.cu:229-239):
 // signed floats ordered through an order-preserving integer key.
 __device__ __forceinline__ unsigned f2key(float f)
@@ -624,7 +813,7 @@ __device__ __forceinline__ void b_col_r(const JobDev *jobs, const WorkItem wi)
     for (int m = 0; m < 8; ++m) {
         const float mod = ok ? J.M[(size_t)(l + m * Q) * W + x] : 0.f;
         float nrm = cnorm_ref(v[m]);
-        if (nrm == 0.f) nrm = 1.f;
+        if (nrm == 0.f && J.mode == kModeShrinkWrap) nrm = 1.f;
         const float f = __fdiv_rn(mod, nrm);
         v[m] = make_float2(__fmul_rn(v[m].x, f), __fmul_rn(v[m].y, f));
     }
@@ -641,7 +830,7 @@ __global__ void __launch_bounds__(rcol_threads(N)) k_col_r(const JobDev *jobs, c
 }
 
 // row pass: inverse row FFT, HIO update, forward row FFT (see k_row_hio)
-template <bool FIRST, int N>
+template <bool FIRST, int N, bool FIX = false>
 __device__ __forceinline__ void b_row_hio_r(const JobDev *jobs, const WorkItem wi)
 {
     extern __shared__ float4 smem4[];
@@ -660,7 +849,11 @@ __device__ __forceinline__ void b_row_hio_r(const JobDev *jobs, const WorkItem w
     reg_fft<N, rrow_nb(N), false, +1>(v, sm, b, l, J.prow.tw);
     const float beta = J.beta;
     const float thr = st->thr;
-    const bool init_gprev = FIRST && st->hio_cycle == 0;
+    const int k = FIX ? st->cycle : 0;
+    const bool init_gprev = FIX ? k == 0 : FIRST && st->hio_cycle == 0;
+    const bool fin = FIX && k >= J.n_cycles;
+    const bool track = FIX && (J.target > 0.f || fin);
+    double tot = 0.0, cnt = 0.0;
     if (ok) {
 #pragma unroll
         for (int m = 0; m < 8; ++m) {
@@ -673,9 +866,11 @@ __device__ __forceinline__ void b_row_hio_r(const JobDev *jobs, const WorkItem w
             } else {
                 msk = J.mask[idx];
             }
+            if (FIX && track) hio_track(J, idx, gp1, msk, tot, cnt);
+            if (fin) continue;
             const float2 gp = init_gprev ? gp1 : J.G[idx];
             float2 g;
-            if (msk || gp1.x < 0.f)
+            if ((FIX ? msk == 1 : msk != 0) || gp1.x < 0.f)
                 g = make_float2(__fsub_rn(gp.x, __fmul_rn(beta, gp1.x)),
                                 __fsub_rn(gp.y, __fmul_rn(beta, gp1.y)));
             else
@@ -684,16 +879,19 @@ __device__ __forceinline__ void b_row_hio_r(const JobDev *jobs, const WorkItem w
             v[m] = g;
         }
     }
-    reg_fft<N, rrow_nb(N), false, -1>(v, sm, b, l, J.prow.tw);
-    if (ok) {
+    if (!fin) {
+        reg_fft<N, rrow_nb(N), false, -1>(v, sm, b, l, J.prow.tw);
+        if (ok) {
 #pragma unroll
-        for (int m = 0; m < 8; ++m) J.X[base + l + m * Q] = v[m];
+            for (int m = 0; m < 8; ++m) J.X[base + l + m * Q] = v[m];
+        }
     }
+    if (FIX) hio_tile_done<rrow_threads(N)>(J, wi.tile, tot, cnt);
 }
-template <bool FIRST, int N>
+template <bool FIRST, int N, bool FIX = false>
 __global__ void __launch_bounds__(rrow_threads(N)) k_row_hio_r(const JobDev *jobs, const WorkList *L)
 {
-    IMR_ITEM_LOOP((b_row_hio_r<FIRST, N>(jobs, wi)));
+    IMR_ITEM_LOOP((b_row_hio_r<FIRST, N, FIX>(jobs, wi)));
 }
 
 // once per cycle: inverse row FFT -> g'; out, error sums, |g'| blurred along rows
@@ -829,7 +1027,8 @@ __device__ __forceinline__ bool job_live(const JobDev *jobs, const WorkList *L, 
     return jobs[wi.job].st->stop == 0;
 }
 
-template <bool FIRST, int N>
+// FIX: fixed-support HIO iteration (see b_row_hio)
+template <bool FIRST, int N, bool FIX = false>
 __global__ void __launch_bounds__(rrow_threads(N)) k_row_hio_p(const JobDev *jobs, const WorkList *L)
 {
     extern __shared__ __align__(128) unsigned char sbuf[];
@@ -901,7 +1100,11 @@ __global__ void __launch_bounds__(rrow_threads(N)) k_row_hio_p(const JobDev *job
         reg_fft_1buf<N, RowSwz<N, NB>, +1>(v, sX, b, l, rtw);
         const float beta = J.beta;
         const float thr = st->thr;
-        const bool init_gprev = FIRST && st->hio_cycle == 0;
+        const int kit = FIX ? st->cycle : 0;
+        const bool init_gprev = FIX ? kit == 0 : FIRST && st->hio_cycle == 0;
+        const bool fin = FIX && kit >= J.n_cycles;
+        const bool track = FIX && ok && (J.target > 0.f || fin);
+        double tot = 0.0, cnt = 0.0;
 #pragma unroll
         for (int m = 0; m < V; ++m) {
             const int e = b * N + l + m * Q;
@@ -909,24 +1112,30 @@ __global__ void __launch_bounds__(rrow_threads(N)) k_row_hio_p(const JobDev *job
             uint8_t msk;
             if constexpr (FIRST) msk = reinterpret_cast<const float *>(stg + 2 * XB)[e] < thr ? 1 : 0;
             else msk = (stg + 2 * XB)[e];
+            if constexpr (FIX) {
+                if (track) hio_track(J, base + l + m * Q, gp1, msk, tot, cnt);
+            }
             const float2 gp = init_gprev ? gp1 : sG[e];
             float2 g;
-            if (msk || gp1.x < 0.f)
+            if ((FIX ? msk == 1 : msk != 0) || gp1.x < 0.f)
                 g = make_float2(__fsub_rn(gp.x, __fmul_rn(beta, gp1.x)),
                                 __fsub_rn(gp.y, __fmul_rn(beta, gp1.y)));
             else
                 g = gp1;
-            if (ok) {
+            if (ok && !fin) {
                 J.G[base + l + m * Q] = g;
                 if constexpr (FIRST) J.mask[base + l + m * Q] = msk;
             }
             v[m] = g;
         }
-        reg_fft_1buf<N, RowSwz<N, NB>, -1>(v, sX, b, l, rtw);
-        if (ok) {
+        if (!fin) {
+            reg_fft_1buf<N, RowSwz<N, NB>, -1>(v, sX, b, l, rtw);
+            if (ok) {
 #pragma unroll
-            for (int m = 0; m < V; ++m) J.X[base + l + m * Q] = v[m];
+                for (int m = 0; m < V; ++m) J.X[base + l + m * Q] = v[m];
+            }
         }
+        if constexpr (FIX) hio_tile_done<rrow_threads(N)>(J, wi.tile, tot, cnt);
         fence_proxy_async_smem();
         __syncthreads();   // stage s is free for the copy issued next iteration
         item = nxt;
@@ -1027,7 +1236,7 @@ __global__ void __launch_bounds__(rcol_threads(N)) k_col_p(const JobDev *jobs, c
             if constexpr (TM) mod = reinterpret_cast<const float *>(stg + XB)[(l + m * Q) * NB + b];
             else mod = ok ? J.M[(size_t)(l + m * Q) * W + x] : 0.f;
             float nrm = cnorm_ref(v[m]);
-            if (nrm == 0.f) nrm = 1.f;
+            if (nrm == 0.f && J.mode == kModeShrinkWrap) nrm = 1.f;
             const float f = __fdiv_rn(mod, nrm);
             v[m] = make_float2(__fmul_rn(v[m].x, f), __fmul_rn(v[m].y, f));
         }

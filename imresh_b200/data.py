@@ -126,3 +126,20 @@ def cfg4_specs(n: int = 20000, seed: int = 4):
         ph = float(10 ** rng.uniform(6, 9))
         specs.append(BlobSpec(W, H, nb, 0.15 * min(W, H), (1.0, 3.0), (0.3, 1.0), ph))
     return specs
+
+
+# ---- inputs of the fixed-support HIO (libs::hybridInputOutput)
+def centrosymmetric(M: np.ndarray) -> np.ndarray:
+    """max(M[k], M[-k]) per frequency: exactly centrosymmetric, as the
+    modulus of a real object is (the reference's debug build asserts it,
+    src/imresh/libs/hybridInputOutput.cpp:140-158)."""
+    return np.maximum(M, np.roll(np.flip(M), 1, axis=(0, 1)))
+
+
+def support_mask(spec: BlobSpec, margin: float = 1.5) -> np.ndarray:
+    """uint8 [H, W]: 1 outside a centred disk that holds every blob centre's
+    disk plus `margin` blob widths (the fixed support of the HIO)."""
+    W, H = spec.width, spec.height
+    r = spec.radius + margin * 5.0 * spec.sigma[1]
+    yy, xx = np.mgrid[:H, :W]
+    return (((xx - W / 2.0) ** 2 + (yy - H / 2.0) ** 2) > r * r).astype(np.uint8)

@@ -138,6 +138,60 @@ int imr_diffraction_intensity(float *h_io, unsigned W, unsigned H, void *stream)
  * the result goes to HOST *h_max; synchronous. */
 int imr_vector_max(const float *d_data, size_t n, float *h_max, void *stream);
 
+/* Mask element types of imr_calculate_hio_error. */
+#define IMR_MASK_F32 0
+#define IMR_MASK_U8 1
+/* HIO error of n complex64 values (cudaCalculateHioError<cufftComplex, float>,
+ * src/imresh/algorithms/cuda/cudaVectorReduce.cu:357-403, hpp:160-170):
+ * total = sum w*|z|, count = sum w, error = sqrtf(total)/count, with
+ * w = (mask != 0) xor invert_mask.  Sums in double, rounded to float once.
+ * Results go to HOST pointers (any may be NULL); synchronous. */
+int imr_calculate_hio_error(const void *d_data, const void *d_mask, int mask_type, size_t n,
+                            int invert_mask, float *h_total, float *h_count, float *h_error,
+                            void *stream);
+
+/* ------------------------------------------------------------------------
+ * Fixed-support hybrid input-output with a random initial phase
+ * (imresh::libs::hybridInputOutput, src/imresh/libs/hybridInputOutput.cpp:193-306,
+ * hpp:81-90), on the engine's fused passes.
+ *
+ * io: HOST W*H floats, the Fourier modulus in, Re(g') out.  mask: HOST W*H
+ * bytes, 1 = outside the support (HIO applies where mask == 1; the error
+ * weighs |g'| by the mask value).  nCycles == 0 means unbounded (the
+ * reference's UINT_MAX); beta <= 0 means 0.9; targetError <= 0 disables the
+ * per-iteration error test.  The initial phase is the argument of the 2D FFT
+ * of the C library's rand() numbers after srand(IMR_HIO_SEED), as in the
+ * reference (cpp:160-167), drawn on the GPU.  Synchronous. */
+#define IMR_HIO_SEED 2623091912u
+int imr_hybrid_input_output(float *io, const unsigned char *mask, unsigned W, unsigned H,
+                            unsigned nCycles, float targetError, float beta, void *stream);
+
+/* The C library's numbers after srand(seed), as n DEVICE complex64 values
+ * ((float)rand()/RAND_MAX, 0): the random real field of addRandomPhase
+ * (hybridInputOutput.cpp:160-167), drawn in parallel by jumping glibc's
+ * additive feedback generator ahead.  seed 0 acts as 1, as in glibc.
+ * Asynchronous on `stream`. */
+int imr_rand_field(void *d_out, size_t n, unsigned seed, void *stream);
+
+/* The same as a reusable plan over DEVICE buffers (no allocation or graph
+ * capture per call).  execute is asynchronous on `stream`; execute_host takes
+ * HOST buffers and returns after the result is copied back.  seed: the
+ * srand() seed of the initial phase (IMR_HIO_SEED for the reference's).
+ * stats: iterations = HIO updates applied before the returned g', the last
+ * tested error, and the per-iteration errors (up to cap values; iterations
+ * whose error was not tested read 0). */
+typedef struct imr_hio_plan imr_hio_plan;
+int imr_hio_plan_create(imr_hio_plan **plan, unsigned W, unsigned H, unsigned nCycles,
+                        float targetError, float beta);
+int imr_hio_plan_execute(imr_hio_plan *plan, const float *d_modulus, const unsigned char *d_mask,
+                         float *d_out, unsigned seed, void *stream);
+int imr_hio_plan_execute_host(imr_hio_plan *plan, const float *h_modulus,
+                              const unsigned char *h_mask, float *h_out, unsigned seed,
+                              void *stream);
+int imr_hio_plan_stats(imr_hio_plan *plan, void *stream, int *iterations, float *last_error,
+                       float *errors, int cap);
+int imr_hio_plan_destroy(imr_hio_plan *plan);
+
 /* ------------------------------------------------------------------------
  * Reconstruction that allocates nothing -- no counterpart in the reference.
  * For callers that cannot call cudaMalloc (memory owned by a fixed arena or a

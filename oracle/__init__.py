@@ -3,8 +3,9 @@
 ctypes front end to two CPU libraries:
 
 * ``liboracle.so`` -- this project's C restatement of the reference's CPU
-  shrink-wrap path (float and FP64) over the project-written FFT
-  (``shrinkwrap_oracle.c``, ``imro_fft.c``);
+  shrink-wrap path and of its fixed-support random-phase HIO (float and FP64)
+  over the project-written FFT (``shrinkwrap_oracle.c``, ``hio_oracle.c``,
+  ``imro_fft.c``);
 * ``_ref/libimresh_ref.so`` -- the reference's own CPU ``shrinkWrap`` and the
   functions it calls, compiled unmodified from its sources over the FFTW shim
   (``Makefile`` target ``ref``; present only where it was built).
@@ -36,6 +37,11 @@ def build(ref: bool = True) -> None:
     if ref and os.path.isdir(os.environ.get("IMRESH_REF", "/root/reference")):
         subprocess.run(["make", "-s", "-C", _HERE, "ref",
                         "REF=" + os.environ.get("IMRESH_REF", "/root/reference")], check=True)
+
+
+class _HioTrace(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("last_error", C.c_float), ("errors", C.c_void_p),
+                ("errors_cap", C.c_int)]
 
 
 class _Trace(C.Structure):
@@ -72,6 +78,12 @@ def lib():
                    C.c_float, C.c_float, C.c_float, C.c_uint, C.POINTER(_Trace)]
         L.imro_shrinkwrap_f32.argtypes = [_f32p] + sw_args
         L.imro_shrinkwrap_f64.argtypes = [_f64p] + sw_args
+        u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+        hio_args = [u8p, C.c_uint, C.c_uint, C.c_uint, C.c_float, C.c_float, C.c_uint,
+                    C.POINTER(_HioTrace)]
+        L.imro_hio_f32.argtypes = [_f32p] + hio_args
+        L.imro_hio_f64.argtypes = [_f64p] + hio_args
+        L.imro_random_phase_f32.argtypes = [_f32p, _f32p, C.c_uint, C.c_uint, C.c_uint]
         _LIB = L
     return _LIB
 
@@ -97,6 +109,9 @@ def ref_lib():
         L.imro_ref_hio_error.argtypes = [_f32p, _f32p, C.c_uint,
                                          C.POINTER(C.c_float), C.POINTER(C.c_float)]
         L.imro_ref_hio_error.restype = C.c_float
+        L.imro_ref_hio.argtypes = [_f32p, np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS"),
+                                   C.c_uint, C.c_uint, C.c_uint, C.c_float, C.c_float]
+        L.imro_ref_hio.restype = C.c_int
         _REF = L
     return _REF
 
@@ -223,4 +238,65 @@ def ref_shrinkwrap(modulus: np.ndarray, p: SwParams) -> np.ndarray:
     rc = L.imro_ref_shrinkwrap(io, W, H, *p.args())
     if rc != 0:
         raise RuntimeError(f"reference shrinkWrap returned {rc}")
+    return io.reshape(H, W)
+
+
+# ---------------------------------------------------------------- fixed-support HIO
+HIO_SEED = 2623091912   # srand() seed of addRandomPhase (hybridInputOutput.cpp:160)
+
+
+@dataclass
+class HioResult:
+    out: np.ndarray
+    iterations: int
+    last_error: float
+    errors: np.ndarray
+
+
+def hio(modulus: np.ndarray, mask: np.ndarray, n_cycles: int = 0, target_error: float = 1e-6,
+        beta: float = 0.9, seed: int = HIO_SEED, fp64: bool = False, errors_cap: int = 4096) -> HioResult:
+    """The restated hybridInputOutput; modulus float [H, W], mask uint8 [H, W]."""
+    H, W = modulus.shape
+    m = np.ascontiguousarray(mask, dtype=np.uint8).reshape(-1)
+    errs = np.zeros(errors_cap, np.float32)
+    tr = _HioTrace(0, 0.0, errs.ctypes.data, errors_cap)
+    if fp64:
+        io = np.ascontiguousarray(modulus, dtype=np.float64).reshape(-1).copy()
+        lib().imro_hio_f64(io, m, W, H, n_cycles, target_error, beta, seed, C.byref(tr))
+    else:
+        io = np.ascontiguousarray(modulus, dtype=np.float32).reshape(-1).copy()
+        lib().imro_hio_f32(io, m, W, H, n_cycles, target_error, beta, seed, C.byref(tr))
+    return HioResult(io.reshape(H, W), tr.iterations, tr.last_error,
+                     errs[:min(tr.iterations + 1, errors_cap)])
+
+
+def random_phase(modulus: np.ndarray, seed: int = HIO_SEED) -> np.ndarray:
+    """addRandomPhase: complex64 [H, W] = M e^{i phase}."""
+    H, W = modulus.shape
+    m = np.ascontiguousarray(modulus, dtype=np.float32).reshape(-1)
+    out = np.zeros(2 * m.size, np.float32)
+    lib().imro_random_phase_f32(m, out, W, H, seed)
+    return out.view(np.complex64).reshape(H, W)
+
+
+def rand_field(n: int, seed: int = HIO_SEED) -> np.ndarray:
+    """The C library's (float)rand()/RAND_MAX sequence after srand(seed)."""
+    libc = C.CDLL(None)
+    libc.srand(C.c_uint(seed))
+    r = np.fromiter((libc.rand() for _ in range(n)), dtype=np.int64, count=n)
+    return (r.astype(np.float32) / np.float32(2147483647.0)).astype(np.float32)
+
+
+def ref_hio(modulus: np.ndarray, mask: np.ndarray, n_cycles: int = 0, target_error: float = 1e-6,
+            beta: float = 0.9) -> np.ndarray:
+    """The reference's own hybridInputOutput (oracle/_ref); raises if not built."""
+    L = ref_lib()
+    if L is None:
+        raise RuntimeError("oracle/_ref/libimresh_ref.so is not built")
+    H, W = modulus.shape
+    io = np.ascontiguousarray(modulus, dtype=np.float32).reshape(-1).copy()
+    m = np.ascontiguousarray(mask, dtype=np.uint8).reshape(-1)
+    rc = L.imro_ref_hio(io, m, W, H, n_cycles, target_error, beta)
+    if rc != 0:
+        raise RuntimeError(f"reference hybridInputOutput returned {rc}")
     return io.reshape(H, W)

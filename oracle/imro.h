@@ -69,6 +69,24 @@ int imro_shrinkwrap_f64(double *io, unsigned W, unsigned H, unsigned nCycles,
                         float sigma0, float sigmaChange, unsigned nHio,
                         imro_sw_trace *trace);
 
+/* ---- fixed-support HIO with a random initial phase ------------------------
+ * hybridInputOutput / addRandomPhase (src/imresh/libs/hybridInputOutput.cpp:126-306):
+ * io: W*H modulus in, Re(g') out; mask: W*H bytes, 1 = outside the support.
+ * nCycles 0 = unbounded, beta <= 0 = 0.9, targetError <= 0 = no error test.
+ * The random field is the C library's rand() after srand(seed). */
+typedef struct imro_hio_trace {
+    int iterations;        /* HIO updates applied before the returned g'   */
+    float last_error;      /* last error evaluated                         */
+    float *errors;         /* [errors_cap] error of each tested g', or NULL */
+    int errors_cap;
+} imro_hio_trace;
+int imro_hio_f32(float *io, const unsigned char *mask, unsigned W, unsigned H, unsigned nCycles,
+                 float targetError, float beta, unsigned seed, imro_hio_trace *trace);
+int imro_hio_f64(double *io, const unsigned char *mask, unsigned W, unsigned H, unsigned nCycles,
+                 float targetError, float beta, unsigned seed, imro_hio_trace *trace);
+/* addRandomPhase alone: out = W*H interleaved complex M e^{i phase}. */
+void imro_random_phase_f32(const float *mod, float *out, unsigned W, unsigned H, unsigned seed);
+
 #ifdef __cplusplus
 }
 #endif

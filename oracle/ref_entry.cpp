@@ -16,6 +16,11 @@
  *                               (src/imresh/algorithms/vectorReduce.cpp:73-87)
  *   imro_ref_hio_error       -> imresh::libs::calculateHioError<fftwf_complex,float>
  *                               (src/imresh/libs/hybridInputOutput.cpp:67-103)
+ *   imro_ref_hio             -> imresh::libs::hybridInputOutput
+ *                               (src/imresh/libs/hybridInputOutput.cpp:193-306);
+ *                               rSize = {H, W}: the FFTW plan's slow then fast
+ *                               dimension (cpp:219-222); rnCores = 0 leaves the
+ *                               process's OpenMP thread count alone
  */
 #include <fftw3.h>
 #include "algorithms/shrinkWrap.hpp"
@@ -64,6 +69,13 @@ float imro_ref_hio_error(const float *gp, const float *mask, unsigned n,
 {
     return imresh::libs::calculateHioError<fftwf_complex, float>(
         (const fftwf_complex *)gp, mask, n, false, total, count);
+}
+
+int imro_ref_hio(float *io, const unsigned char *mask, unsigned W, unsigned H, unsigned nCycles,
+                 float targetError, float beta)
+{
+    return imresh::libs::hybridInputOutput(io, mask, std::vector<unsigned>{H, W}, nCycles,
+                                           targetError, beta, 0);
 }
 
 }

@@ -2,8 +2,11 @@
 // it (examples/miniExample.cpp:102-116, examples/threadedExample.cpp:44-113):
 // build an object, turn it into a Fourier modulus with diffractionIntensity,
 // reconstruct it with cudaShrinkWrap, then run a batch through the task
-// queue.  Compiled against include/imresh (the reference's header paths) and
-// linked against libimresh_b200.so only.  Prints "OK" on success.
+// queue; then the fixed-support HIO (libs::hybridInputOutput) and the device
+// reductions of algorithms/cuda/cudaVectorReduce.hpp on buffers the caller
+// allocates.  Compiled against include/imresh (the reference's header paths)
+// and linked against libimresh_b200.so (plus the CUDA runtime for the
+// caller's own cudaMalloc).  Prints "OK" on success.
 #include <atomic>
 #include <cmath>
 #include <cstdio>
@@ -11,7 +14,11 @@
 #include <string>
 #include <vector>
 
+#include <cuda_runtime.h>
+
 #include "algorithms/cuda/cudaShrinkWrap.hpp"
+#include "algorithms/cuda/cudaVectorReduce.hpp"
+#include "libs/hybridInputOutput.hpp"
 #include "io/taskQueue.cu"
 #include "io/writeOutFuncs/writeOutFuncs.hpp"
 #include "libs/diffractionIntensity.hpp"
@@ -73,6 +80,49 @@ int main()
     imresh::io::taskQueueDeinit();
     if (finished != nTasks || bad != 0) {
         std::printf("task queue: finished %d of %d, bad %d\n", (int)finished, nTasks, (int)bad);
+        return 1;
+    }
+    // hybridInputOutput: fixed disk support, 30 iterations, no error test
+    std::vector<float> io(modulus);
+    std::vector<uint8_t> mask(W * H);
+    for (unsigned y = 0; y < H; ++y)
+        for (unsigned x = 0; x < W; ++x) {
+            const float dx = x - 0.5f * W, dy = y - 0.5f * H;
+            mask[y * W + x] = dx * dx + dy * dy > 40.f * 40.f ? 1 : 0;
+        }
+    rc = imresh::libs::hybridInputOutput(io.data(), mask.data(), std::vector<unsigned>{H, W}, 30, 0.f);
+    if (rc != 0 || !finite(io.data(), io.size())) {
+        std::printf("hybridInputOutput failed: rc=%d\n", rc);
+        return 1;
+    }
+    if (imresh::libs::hybridInputOutput(io.data(), mask.data(), std::vector<unsigned>{H}, 3) != 1) {
+        std::printf("hybridInputOutput accepted a 1D size\n");
+        return 1;
+    }
+
+    // device reductions: (3, 4) where masked -> total = 5 * count
+    const unsigned n = 4096;
+    std::vector<float> hz(2 * n), hm(n);
+    for (unsigned i = 0; i < n; ++i) {
+        hm[i] = (i % 3 == 0) ? 1.f : 0.f;
+        hz[2 * i] = hm[i] ? 3.f : 0.25f;
+        hz[2 * i + 1] = hm[i] ? 4.f : 0.5f;
+    }
+    float *dz = nullptr, *dm = nullptr;
+    if (cudaMalloc(&dz, sizeof(float) * 2 * n) != cudaSuccess || cudaMalloc(&dm, sizeof(float) * n) != cudaSuccess) {
+        std::printf("cudaMalloc failed\n");
+        return 1;
+    }
+    cudaMemcpy(dz, hz.data(), sizeof(float) * 2 * n, cudaMemcpyHostToDevice);
+    cudaMemcpy(dm, hm.data(), sizeof(float) * n, cudaMemcpyHostToDevice);
+    float total = 0, count = 0;
+    const float err = imresh::algorithms::cuda::cudaCalculateHioError((const float2 *)dz, (const float *)dm, n,
+                                                                      false, cudaStream_t(0), &total, &count);
+    const float mx = imresh::algorithms::cuda::cudaVectorMax((const float *)dz, 2 * n);
+    cudaFree(dz);
+    cudaFree(dm);
+    if (count != 1366.f || total != 5.f * count || !(err > 0) || mx != 4.f) {
+        std::printf("reductions: count %g total %g err %g max %g\n", count, total, err, mx);
         return 1;
     }
     std::printf("OK\n");

@@ -1,5 +1,6 @@
 """Helper for the tests: compile tests/cpp/drop_in.cpp against the
-reference-path headers in include/imresh and libimresh_b200.so."""
+reference-path headers in include/imresh and libimresh_b200.so (and the CUDA
+runtime, for the program's own device buffers)."""
 import os
 import subprocess
 
@@ -12,6 +13,7 @@ def build_drop_in(out_dir: str) -> str:
     cmd = ["g++", "-std=c++14", "-O1", "-I", os.path.join(ROOT, "include", "imresh"),
            "-I", os.path.join(ROOT, "include"), "-I", "/usr/local/cuda/include",
            os.path.join(ROOT, "tests", "cpp", "drop_in.cpp"), "-L", lib_dir, "-limresh_b200",
-           "-Wl,-rpath," + lib_dir, "-lpthread", "-o", exe]
+           "-Wl,-rpath," + lib_dir, "-L", "/usr/local/cuda/lib64", "-lcudart",
+           "-Wl,-rpath,/usr/local/cuda/lib64", "-lpthread", "-o", exe]
     subprocess.run(cmd, check=True, capture_output=True, text=True)
     return exe

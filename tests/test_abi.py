@@ -66,5 +66,6 @@ def test_reference_symbols_exported():
     out = subprocess.run(["nm", "-DC", imr.LIB_PATH], capture_output=True, text=True).stdout
     for sym in ("imresh::algorithms::cuda::cudaShrinkWrap(", "imresh::io::taskQueueInit()",
                 "imresh::io::taskQueueDeinit()", "imresh::io::addTask(",
-                "imresh::io::writeOutFuncs::justFree(", "imresh::libs::diffractionIntensity("):
+                "imresh::io::writeOutFuncs::justFree(", "imresh::libs::diffractionIntensity(",
+                "imresh::libs::hybridInputOutput("):
         assert sym in out, sym

@@ -210,3 +210,59 @@ def test_fp64_oracle_is_close_at_short_horizon():
     a = oracle.shrinkwrap(M, p).out
     b = oracle.shrinkwrap(M, p, fp64=True).out
     assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-5
+
+
+# ------------------------------------------------------------------ fixed-support HIO
+def _hio_case(H, W, seed=3):
+    spec = data.BlobSpec(W, H, 8, min(W, H) / 6.0, (1.5, 2.0), (0.5, 1.0), None)
+    M, _ = data.make_modulus(spec, seed)
+    return data.centrosymmetric(M), data.support_mask(spec)
+
+
+def test_rand_field_is_the_c_library_stream():
+    """The oracle's random field is srand(2623091912)/rand() itself, checked
+    against glibc's published additive feedback generator restated here."""
+    f = oracle.rand_field(400)
+    r = [2623091912 - (1 << 32)]
+    for i in range(1, 31):
+        r.append((16807 * r[i - 1]) % 2147483647)
+    r = [x & 0xFFFFFFFF for x in r]
+    r += [r[i - 31] for i in range(31, 34)]
+    for i in range(34, 344 + 400):
+        r.append((r[i - 31] + r[i - 3]) & 0xFFFFFFFF)
+    want = (np.array([x >> 1 for x in r[344:]], np.int64).astype(np.float32)
+            / np.float32(2147483647.0))
+    np.testing.assert_array_equal(f, want)
+
+
+@pytest.mark.parametrize("shape,n,target", [((48, 64), 1, 0.0), ((48, 64), 5, 0.0),
+                                            ((64, 64), 30, -1.0), ((30, 42), 12, 0.0),
+                                            ((1, 8), 3, 0.0), ((48, 64), 3, 1e30),
+                                            ((17, 24), 7, 0.0)])
+def test_restated_hio_bitexact_vs_reference(shape, n, target):
+    _ref_or_skip()
+    M, mask = _hio_case(*shape)
+    ours = oracle.hio(M, mask, n, target, 0.9)
+    ref = oracle.ref_hio(M, mask, n, target, 0.9)
+    np.testing.assert_array_equal(ours.out, ref)
+    assert ours.iterations == (0 if target > 1 else n)
+
+
+def test_restated_hio_stops_like_reference():
+    _ref_or_skip()
+    M, mask = _hio_case(64, 64, seed=5)
+    errs = oracle.hio(M, mask, 60, 1e-30, 0.9).errors
+    # first new minimum that beats every earlier error by a clear margin
+    k = next(k for k in range(5, 60) if errs[k] < 0.98 * errs[:k].min())
+    target = float(0.5 * (errs[k] + errs[:k].min()))
+    ours = oracle.hio(M, mask, 60, target, 0.9)
+    assert ours.iterations == k
+    np.testing.assert_array_equal(ours.out, oracle.ref_hio(M, mask, 60, target, 0.9))
+
+
+def test_hio_defaults_follow_reference():
+    """beta <= 0 selects 0.9 (hybridInputOutput.cpp:209)."""
+    M, mask = _hio_case(32, 32)
+    a = oracle.hio(M, mask, 4, 0.0, 0.9).out
+    np.testing.assert_array_equal(oracle.hio(M, mask, 4, 0.0, 0.0).out, a)
+    np.testing.assert_array_equal(oracle.hio(M, mask, 4, 0.0, -1.0).out, a)
