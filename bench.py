@@ -389,7 +389,8 @@ def run_ours(args, rank, world, local_rank):
     try:   # DRAM bytes per launch of the dominant kernel, from the committed ncu capture
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
             tj = json.load(f)
-        traffic = tj.get("k_row_hio_p<0,2048>" if dom[0] == "row" else "k_col_p<2048>")
+        entry = tj.get("row_pass_2048" if dom[0] == "row" else "col_pass_2048")
+        traffic = entry["dram_bytes_per_launch"] if entry else None
     except Exception:
         pass
     iter_gbs = (row_b + col_b) / ((ms_row + ms_col) * 1e-3) / 1e9
@@ -419,7 +420,7 @@ def run_ours(args, rank, world, local_rank):
         "roofline": {"bound": "hbm", "achieved": dom[3], "peak": peak, "unit": "GB/s",
                      "frac": dom[3] / peak, "traffic": traffic,
                      "traffic_source": "profiles/traffic.json (ncu, cold cache, per launch)",
-                     "kernel": f"{dom[0]} pass ({'k_row_hio' if dom[0] == 'row' else 'k_col'})",
+                     "kernel": f"{dom[0]} pass ({'k_row_hio_p<false,2048>' if dom[0] == 'row' else 'k_col_p16<2048,4>'})",
                      "peak_source": peak_kind,
                      "algorithmic_bytes_per_launch": dom[1], "ms_per_launch": dom[2],
                      "row_pass_gbs": row_gbs, "col_pass_gbs": col_gbs,

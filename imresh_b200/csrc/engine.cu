@@ -245,17 +245,22 @@ static RowKernels row_set()
 template <int N>
 static ColKernels col_set()
 {
-    if constexpr (N >= 16 && is_pow2(N))
+    if constexpr (N >= 128 && N <= 4096 && is_pow2(N)) {   // 16 values per thread in the pipelined pass
+        constexpr int T = pcol16_nbt(N);
+        return ColKernels{k_col_r<N>, k_col_init_r<N>, k_fft_cols_r<-1, N>, k_fft_cols_r<+1, N>,
+                          rcol_nb(N), rcol_threads(N), rcol_smem(N), k_col_p16<N, T>, pcol16_smem<N, T>(),
+                          pcol_box_rows(N), T * 4 >= 16 ? 1 : 0, pcol16_threads(N, T), 0, T};
+    } else if constexpr (N >= 16 && is_pow2(N))
         return ColKernels{k_col_r<N>, k_col_init_r<N>, k_fft_cols_r<-1, N>, k_fft_cols_r<+1, N>,
                           rcol_nb(N), rcol_threads(N), rcol_smem(N), k_col_p<N>, pcol_smem<N>(),
-                          pcol_box_rows(N), pcol_tma_m(N) ? 1 : 0, pcol_threads(N), 0};
+                          pcol_box_rows(N), pcol_tma_m(N) ? 1 : 0, pcol_threads(N), 0, rcol_nb(N)};
     else if constexpr (N >= 8 && is_pow2(N))
         return ColKernels{k_col_r<N>, k_col_init_r<N>, k_fft_cols_r<-1, N>, k_fft_cols_r<+1, N>,
                           rcol_nb(N), rcol_threads(N), rcol_smem(N), nullptr, 0, 0, 0, 0, 0};
     else if constexpr (is_3pow2(N))
         return ColKernels{k_col<N>, k_col_init<N>, k_fft_cols<-1, N>, k_fft_cols<+1, N>, col_nb(N),
                           col_threads(N), 0, k_col_p<N>, pcol_smem<N>(), pcol_box_rows(N),
-                          pcol_tma_m(N) ? 1 : 0, pcol_threads(N), 0};
+                          pcol_tma_m(N) ? 1 : 0, pcol_threads(N), 0, rcol_nb(N)};
     else
         return ColKernels{k_col<N>, k_col_init<N>, k_fft_cols<-1, N>, k_fft_cols<+1, N>, col_nb(N),
                           col_threads(N), 0, nullptr, 0, 0, 0, 0, N < 0 ? -N : 0};
@@ -546,8 +551,8 @@ int job_prepare(unsigned W, unsigned H, const imr_params &p, JobDev &J, JobShape
     J.rpc = S.rk.nb < J.H ? S.rk.nb : J.H;
     J.cpc = S.ck.nb < J.W ? S.ck.nb : J.W;
     S.p_rows = S.rk.p_hio != nullptr;
-    S.p_cols = S.ck.p_col != nullptr && J.W % 4 == 0 && J.W >= S.ck.nb;
-    if (S.p_cols) J.cpc = S.ck.nb;
+    S.p_cols = S.ck.p_col != nullptr && J.W % 4 == 0 && J.W >= S.ck.p_nb;
+    if (S.p_cols) J.cpc = S.ck.p_nb;
     J.n_row_tiles = (J.H + J.rpc - 1) / J.rpc;
     J.n_col_tiles = (J.W + J.cpc - 1) / J.cpc;
     J.vb_tiles_x = (J.W + kVbTileX - 1) / kVbTileX;
@@ -606,8 +611,8 @@ void job_bind(JobDev &J, JobShape &S, char *a, JobState *st)
     J.use_tma_cols = 0;
     if (S.p_cols) {
         const int br = S.ck.p_box_rows;
-        bool okm = encode_tensor_map(&J.tmX, J.X, J.W, J.H, 8, S.ck.nb, br);
-        if (okm && S.ck.p_tma_m) okm = encode_tensor_map(&J.tmM, J.M, J.W, J.H, 4, S.ck.nb, br);
+        bool okm = encode_tensor_map(&J.tmX, J.X, J.W, J.H, 8, S.ck.p_nb, br);
+        if (okm && S.ck.p_tma_m) okm = encode_tensor_map(&J.tmM, J.M, J.W, J.H, 4, S.ck.p_nb, br);
         if (!okm) {   // shape the TMA unit cannot describe: per-tile column pass
             S.p_cols = false;
             J.cpc = S.ck.nb < J.W ? S.ck.nb : J.W;

@@ -56,6 +56,7 @@ struct ColKernels {
     int p_tma_m;     // 1: the modulus tile also arrives by TMA
     int p_threads;   // threads of the pipelined column pass
     int bs_m;        // Bluestein work length (0: direct transform)
+    int p_nb;        // columns per tile of the pipelined pass (its TMA box width)
 };
 RowKernels row_kernels(int N);
 ColKernels col_kernels(int N);

@@ -88,6 +88,40 @@ __device__ __forceinline__ void dft8(float2 *v)
     v[7] = csub(e[3], o3);
 }
 
+// 16 points as 4 x 4: DFT4 over n1 of x[4 n1 + n2], twiddle W16^(n2 k1),
+// DFT4 over n2; output k1 + 4 k2.
+template <int S>
+__device__ __forceinline__ void dft16(float2 *v)
+{
+    const float c1 = 0.92387953251128675613f, s1 = 0.38268343236508977173f;   // cos, sin(pi/8)
+    const float h = 0.70710678118654752440f;
+    float2 y[4][4];
+#pragma unroll
+    for (int n2 = 0; n2 < 4; ++n2) {
+        float2 a[4] = {v[n2], v[4 + n2], v[8 + n2], v[12 + n2]};
+        dft4<S>(a);
+#pragma unroll
+        for (int k1 = 0; k1 < 4; ++k1) y[n2][k1] = a[k1];
+    }
+    // W16^e = cos(2 pi e/16) + S i sin(2 pi e/16), e = n2*k1 in {1,2,3,4,6,9}
+    y[1][1] = cmul(y[1][1], make_float2(c1, S * s1));
+    y[1][2] = make_float2(h * (y[1][2].x - S * y[1][2].y), h * (S * y[1][2].x + y[1][2].y));
+    y[1][3] = cmul(y[1][3], make_float2(s1, S * c1));
+    y[2][1] = make_float2(h * (y[2][1].x - S * y[2][1].y), h * (S * y[2][1].x + y[2][1].y));
+    y[2][2] = mul_si<S>(y[2][2]);
+    y[2][3] = make_float2(h * (-y[2][3].x - S * y[2][3].y), h * (S * y[2][3].x - y[2][3].y));
+    y[3][1] = cmul(y[3][1], make_float2(s1, S * c1));
+    y[3][2] = make_float2(h * (-y[3][2].x - S * y[3][2].y), h * (S * y[3][2].x - y[3][2].y));
+    y[3][3] = cmul(y[3][3], make_float2(-c1, -S * s1));
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) {
+        float2 b[4] = {y[0][k1], y[1][k1], y[2][k1], y[3][k1]};
+        dft4<S>(b);
+#pragma unroll
+        for (int k2 = 0; k2 < 4; ++k2) v[k1 + 4 * k2] = b[k2];
+    }
+}
+
 template <int S>
 __device__ __forceinline__ void dft3(float2 *v)
 {
@@ -163,6 +197,7 @@ __device__ __forceinline__ void dftR(float2 *v)
     else if constexpr (R == 4) dft4<S>(v);
     else if constexpr (R == 5) dft5<S>(v);
     else if constexpr (R == 7) dft7<S>(v);
+    else if constexpr (R == 16) dft16<S>(v);
     else dft8<S>(v);
 }
 

@@ -344,6 +344,157 @@ __device__ __forceinline__ void reg_fft_1buf(float2 (&v)[reg_v(N)], float2 *buf,
     reg_passes_1buf<N, LAYOUT, S, 0, 1, SMEM_TW>(v, buf, b, l, tw);
 }
 
+// ---- 16 values per thread (powers of two >= 128) -----------------------------
+// Thread l of a sequence holds positions l + m*N/16, m = 0..15; passes of
+// radix 16 first, then one pass of the remaining 2, 4 or 8.  A length-2048
+// transform (16, 16, 8) costs two shared-memory exchanges instead of the
+// three of the 8-value form, and a third fewer barriers.
+__host__ __device__ constexpr RadixList reg16_radix_list(int n)
+{
+    RadixList L{0, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0}};
+    int k = 0;
+    while ((1 << k) < n) ++k;
+    for (; k >= 4; k -= 4) L.r[L.n++] = 16;
+    if (k > 0) L.r[L.n++] = 1 << k;
+    return L;
+}
+__host__ __device__ constexpr int tw16_slots_upto(int N, int P)
+{
+    RadixList L = reg16_radix_list(N);
+    const int Q = N / 16;
+    int slots = 0, ns = 1;
+    for (int p = 0; p < P && p < L.n; ++p) {
+        if (p > 0) slots += (Q % ns == 0) ? 1 : 16 / L.r[p];
+        ns *= L.r[p];
+    }
+    return slots;
+}
+__host__ __device__ constexpr int tw16_slots(int N) { return tw16_slots_upto(N, reg16_radix_list(N).n); }
+
+// Per-thread twiddle powers w, w^2, w^4, w^8 of every butterfly base, read
+// from the length-N table once per kernel (they depend only on l).
+template <int N>
+struct RegTw16 {
+    float2 w[tw16_slots(N) > 0 ? tw16_slots(N) : 1][4];
+
+    template <int P, int NS>
+    __device__ __forceinline__ void load_pass(const float2 *__restrict__ tw, int l)
+    {
+        constexpr RadixList L = reg16_radix_list(N);
+        if constexpr (P < L.n) {
+            constexpr int R = L.r[P];
+            constexpr int Q = N / 16;
+            if constexpr (P > 0) {
+                constexpr int off = tw16_slots_upto(N, P);
+                constexpr int STEP = N / (NS * R);
+                constexpr int NSL = (Q % NS == 0) ? 1 : 16 / R;
+#pragma unroll
+                for (int i = 0; i < NSL; ++i) {
+                    const int t = ((l + i * Q) % NS) * STEP;   // t < N/R: 8t < N for R = 16
+#pragma unroll
+                    for (int e = 0; e < 4; ++e)
+                        w[off + i][e] = (R >> e) > 1 ? __ldg(tw + (((1 << e) * t) & (N - 1))) : make_float2(1.f, 0.f);
+                }
+            }
+            load_pass<P + 1, NS * R>(tw, l);
+        }
+    }
+    __device__ __forceinline__ void load(const float2 *__restrict__ tw, int l) { load_pass<0, 1>(tw, l); }
+};
+
+// u[q] *= w^q, q = 1..R-1, from the table powers p = (w, w^2, w^4, w^8)
+// (conjugated for S > 0); the remaining powers are products of at most three
+// of them.  The empty asm keeps the compiler from hoisting the products out of
+// a work-item loop.
+template <int R, int S>
+__device__ __forceinline__ void twiddle_pow(float2 *u, const float2 (&p)[4])
+{
+    float2 w1 = p[0], w2 = p[1], w4 = p[2], w8 = p[3];
+    asm volatile("" : "+f"(w1.x), "+f"(w1.y), "+f"(w2.x), "+f"(w2.y), "+f"(w4.x), "+f"(w4.y), "+f"(w8.x),
+                 "+f"(w8.y));
+    if (S > 0) {
+        w1.y = -w1.y;
+        w2.y = -w2.y;
+        w4.y = -w4.y;
+        w8.y = -w8.y;
+    }
+    if constexpr (R == 2) {
+        u[1] = cmul(u[1], w1);
+    } else if constexpr (R == 4) {
+        u[1] = cmul(u[1], w1);
+        u[2] = cmul(u[2], w2);
+        u[3] = cmul(u[3], cmul(w1, w2));
+    } else {
+        const float2 w3 = cmul(w1, w2);
+        float2 pw[8] = {make_float2(1.f, 0.f), w1, w2, w3, w4, cmul(w1, w4), cmul(w2, w4), cmul(w3, w4)};
+#pragma unroll
+        for (int q = 1; q < 8; ++q) u[q] = cmul(u[q], pw[q]);
+        if constexpr (R == 16) {
+            u[8] = cmul(u[8], w8);
+#pragma unroll
+            for (int q = 1; q < 8; ++q) u[8 + q] = cmul(u[8 + q], cmul(pw[q], w8));
+        }
+    }
+}
+
+// Swizzle of the 16-value exchanges (column tiles): element e of sequence b
+// at (e ^ ((e >> 4) & (16/NB - 1)))*NB + b; conflict-free for every exchange
+// of the 16-value passes (8-byte accesses per half warp).
+template <int N, int NB>
+struct ColSwz16 {
+    static_assert(NB >= 1 && NB <= 16 && 16 % NB == 0, "column tile width must divide 16");
+    __device__ __forceinline__ static int at(int b, int e) { return (e ^ ((e >> 4) & (16 / NB - 1))) * NB + b; }
+};
+
+template <int N, class LAYOUT, int S, int P, int NS>
+__device__ __forceinline__ void reg16_passes(float2 (&v)[16], float2 *buf, int b, int l, const RegTw16<N> &tw)
+{
+    constexpr RadixList L = reg16_radix_list(N);
+    if constexpr (P < L.n) {
+        constexpr int R = L.r[P];
+        constexpr int BPT = 16 / R;
+        constexpr int Q = N / 16;
+        int kk[BPT];
+#pragma unroll
+        for (int i = 0; i < BPT; ++i) {
+            const int j = l + i * Q;
+            const int k = j % NS;
+            kk[i] = k;
+            float2 u[R];
+#pragma unroll
+            for (int q = 0; q < R; ++q) u[q] = v[i + q * BPT];
+            if constexpr (NS > 1) {
+                constexpr int off = tw16_slots_upto(N, P);
+                twiddle_pow<R, S>(u, tw.w[off + (Q % NS == 0 ? 0 : i)]);
+            }
+            dftR<R, S>(u);
+#pragma unroll
+            for (int q = 0; q < R; ++q) v[i + q * BPT] = u[q];
+        }
+        if constexpr (P + 1 < L.n) {
+            __syncthreads();   // earlier reads of buf are complete
+#pragma unroll
+            for (int i = 0; i < BPT; ++i) {
+                const int j = l + i * Q;
+                const int base = (j - kk[i]) * R + kk[i];
+#pragma unroll
+                for (int q = 0; q < R; ++q) buf[LAYOUT::at(b, base + q * NS)] = v[i + q * BPT];
+            }
+            __syncthreads();
+#pragma unroll
+            for (int m = 0; m < 16; ++m) v[m] = buf[LAYOUT::at(b, l + m * Q)];
+            reg16_passes<N, LAYOUT, S, P + 1, NS * R>(v, buf, b, l, tw);
+        }
+    }
+}
+
+template <int N, class LAYOUT, int S>
+__device__ __forceinline__ void reg16_fft(float2 (&v)[16], float2 *buf, int b, int l, const RegTw16<N> &tw)
+{
+    static_assert(is_pow2(N) && N >= 128 && N <= 4096, "16-value FFT length: 2^k, 128..4096");
+    reg16_passes<N, LAYOUT, S, 0, 1>(v, buf, b, l, tw);
+}
+
 // shared memory (bytes) a register-FFT kernel needs
 __host__ __device__ constexpr int reg_smem_bytes(int N, int NB) { return 2 * NB * (N + N / 8) * 8; }
 

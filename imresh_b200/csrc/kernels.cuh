@@ -1257,4 +1257,125 @@ __global__ void __launch_bounds__(rcol_threads(N)) k_col_p(const JobDev *jobs, c
     if (threadIdx.x == 0) bulk_wait0();
 }
 
+// ---- columns, 16 values per thread (powers of two >= 128) ----------------------
+// The tile, stages and TMA traffic of k_col_p; each thread holds 16 values
+// of its column (a length-2048 transform is three passes, two exchanges),
+// and its twiddle powers stay in registers for the whole persistent loop, so
+// no shared-memory twiddle table (whose strided reads were the pass's bank
+// conflicts) remains.  The next tile is requested after the forward FFT of
+// the current one, when the bulk store that last used its stage has long
+// finished reading it, so the issuing thread does not hold its warp back.
+// (Measured at 2048^2 and kept out: 2-column tiles with two CTAs per SM, 15 %
+// slower; three stages with the modulus fetched into registers, 10 % slower.)
+__host__ __device__ constexpr int pcol16_threads(int N, int NBT) { return NBT * N / 16; }
+__host__ __device__ constexpr int pcol16_nbt(int N) { return rcol_nb(N); }
+template <int N, int NBT>
+__host__ __device__ constexpr int pcol16_stage_bytes()
+{
+    return round128(NBT * N * 8 + (NBT * 4 >= 16 ? NBT * N * 4 : 0));
+}
+template <int N, int NBT>
+__host__ __device__ constexpr int pcol16_smem() { return 128 + 2 * pcol16_stage_bytes<N, NBT>(); }
+__host__ __device__ constexpr int pcol16_min_blocks(int N, int NBT) { return NBT * N / 16 <= 256 ? 2 : 1; }
+
+template <int N, int NBT>
+__global__ void __launch_bounds__(pcol16_threads(N, NBT), pcol16_min_blocks(N, NBT))
+k_col_p16(const JobDev *jobs, const WorkList *L)
+{
+    extern __shared__ __align__(128) unsigned char sbuf[];
+    constexpr int NB = NBT, V = 16, Q = N / V;
+    constexpr int XB = NB * N * 8;
+    constexpr int BR = pcol_box_rows(N);
+    constexpr bool TM = NB * 4 >= 16;   // the modulus tile rows are >= 16 bytes: it comes by TMA too
+    constexpr int STAGE = pcol16_stage_bytes<N, NBT>();
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sbuf);
+    unsigned char *stages = sbuf + 128;
+    const int b = threadIdx.x % NB, l = threadIdx.x / NB;
+    const int n_items = L->n;
+
+    auto next_live = [&](int it) {
+        while (it < n_items && !job_live(jobs, L, it)) it += gridDim.x;
+        return it;
+    };
+    auto issue = [&](int item, int s) {   // one thread
+        const WorkItem wi = item_at(L, item);
+        const JobDev &J = jobs[wi.job];
+        unsigned char *st = stages + s * STAGE;
+        const int x0 = wi.tile * NB;
+        mbar_arrive_expect_tx(&bars[s], (uint32_t)(XB + (TM ? NB * N * 4 : 0)));
+        for (int r0 = 0; r0 < N; r0 += BR) {
+            tma_load_2d(st + (size_t)r0 * NB * 8, &J.tmX, x0, r0, &bars[s]);
+            if constexpr (TM) tma_load_2d(st + XB + (size_t)r0 * NB * 4, &J.tmM, x0, r0, &bars[s]);
+        }
+    };
+
+    if (threadIdx.x == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_fence_init();
+    }
+    int item = next_live(blockIdx.x);
+    // the column length is N for every job of this launch: one set of twiddles
+    RegTw16<N> rtw;
+    if (item < n_items) rtw.load(jobs[item_at(L, item).job].pcol.tw, l);
+    __syncthreads();
+    if (threadIdx.x == 0 && item < n_items) issue(item, 0);
+    for (int k = 0; item < n_items; ++k) {
+        const int nxt = next_live(item + gridDim.x);
+        const int s = k & 1;
+        const WorkItem wi = item_at(L, item);
+        const JobDev &J = jobs[wi.job];
+        const int W = J.W;
+        const int x = wi.tile * NB + b;
+        const bool ok = x < W;
+        float mod[V];
+        if constexpr (!TM) {
+#pragma unroll
+            for (int m = 0; m < V; ++m) mod[m] = ok ? __ldg(J.M + (size_t)(l + m * Q) * W + x) : 0.f;
+        }
+        const bool landed = mbar_wait(&bars[s], (uint32_t)((k >> 1) & 1));
+        if (__syncthreads_or(!landed)) {
+            if (threadIdx.x == 0) {
+                atomicExch(&J.st->err, 1);
+                bulk_wait0();
+            }
+            return;
+        }
+        unsigned char *stg = stages + s * STAGE;
+        float2 *sX = reinterpret_cast<float2 *>(stg);
+        float2 v[V];
+#pragma unroll
+        for (int m = 0; m < V; ++m) v[m] = sX[(l + m * Q) * NB + b];
+        reg16_fft<N, ColSwz16<N, NB>, -1>(v, sX, b, l, rtw);
+        if (threadIdx.x == 0 && nxt < n_items) {
+            bulk_wait_read0();   // the store of the previous item has left stage s^1
+            fence_proxy_async_smem();
+            issue(nxt, s ^ 1);
+        }
+        const bool guard = J.mode == kModeShrinkWrap;
+#pragma unroll
+        for (int m = 0; m < V; ++m) {
+            if constexpr (TM) mod[m] = reinterpret_cast<const float *>(stg + XB)[(l + m * Q) * NB + b];
+            float nrm = cnorm_ref(v[m]);
+            if (nrm == 0.f && guard) nrm = 1.f;
+            const float f = __fdiv_rn(mod[m], nrm);
+            v[m] = make_float2(__fmul_rn(v[m].x, f), __fmul_rn(v[m].y, f));
+        }
+        reg16_fft<N, ColSwz16<N, NB>, +1>(v, sX, b, l, rtw);
+        // the result goes back into the stage (tile layout) and leaves by TMA
+        __syncthreads();
+#pragma unroll
+        for (int m = 0; m < V; ++m) sX[(l + m * Q) * NB + b] = v[m];
+        fence_proxy_async_smem();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const int x0 = wi.tile * NB;
+            for (int r0 = 0; r0 < N; r0 += BR) tma_store_2d(&J.tmX, x0, r0, sX + (size_t)r0 * NB);
+            bulk_commit();
+        }
+        item = nxt;
+    }
+    if (threadIdx.x == 0) bulk_wait0();
+}
+
 }  // namespace imr

@@ -172,7 +172,7 @@ extern "C" int imr_shrink_wrap_noalloc(const float *d_modulus, float *d_out, uns
     J.rpc = rk.nb < J.H ? rk.nb : J.H;
     J.cpc = ck.nb < J.W ? ck.nb : J.W;
     bool p_rows = rk.p_hio != nullptr;
-    bool p_cols = ck.p_col != nullptr && J.W % 4 == 0 && J.W >= ck.nb;
+    bool p_cols = ck.p_col != nullptr && J.W % 4 == 0 && J.W >= ck.p_nb;
     J.X = (float2 *)X;
     J.G = (float2 *)G;
     J.M = d_modulus;
@@ -186,9 +186,9 @@ extern "C" int imr_shrink_wrap_noalloc(const float *d_modulus, float *d_out, uns
     J.errors = d_err;
     J.st = d_st;
     if (p_cols) {
-        J.cpc = ck.nb;
-        p_cols = encode_tensor_map(&J.tmX, J.X, J.W, J.H, 8, ck.nb, ck.p_box_rows) &&
-                 (!ck.p_tma_m || encode_tensor_map(&J.tmM, J.M, J.W, J.H, 4, ck.nb, ck.p_box_rows));
+        J.cpc = ck.p_nb;
+        p_cols = encode_tensor_map(&J.tmX, J.X, J.W, J.H, 8, ck.p_nb, ck.p_box_rows) &&
+                 (!ck.p_tma_m || encode_tensor_map(&J.tmM, J.M, J.W, J.H, 4, ck.p_nb, ck.p_box_rows));
         if (!p_cols) J.cpc = ck.nb < J.W ? ck.nb : J.W;
     }
     J.use_tma_cols = p_cols ? 1 : 0;

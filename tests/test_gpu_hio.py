@@ -10,10 +10,11 @@ Tolerances:
   known answer exactly (total = 5 * count) and agrees with the oracle's double
   sums to float rounding;
 * the reconstruction: within 1e-5 relative L2 of the oracle's float path
-  before any update, 1e-4 after up to five (the phase, FFT and modulus
-  roundings differ by ~1e-7 and HIO amplifies them), iteration counts equal,
-  and at long horizons no farther from the oracle's float path than 10x the
-  oracle's own float-vs-FP64 distance.
+  before any update, and after up to five updates within 1e-4 or, where HIO
+  already amplifies float rounding (256^2 random phase: the oracle's own
+  float and FP64 runs differ by 4e-4 after five), within 10x the oracle's own
+  float-vs-FP64 distance; iteration counts equal; the same yardstick at long
+  horizons.
 """
 import numpy as np
 import pytest
@@ -27,6 +28,15 @@ pytestmark = pytest.mark.gpu
 
 def _rel(a, b):
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def _assert_close_to_oracle(out, ref_out, M, mask, n, seed=imr.HIO_SEED):
+    """Within 1e-4 of the oracle's float path, or within 10x the oracle's own
+    float-vs-FP64 distance where HIO already amplifies float rounding."""
+    d = _rel(out, ref_out)
+    if d >= 1e-4:
+        ref64 = oracle.hio(M, mask, n, 1e-30, 0.9, seed=seed, fp64=True)
+        assert d <= 10 * _rel(ref_out, ref64.out)
 
 
 def _case(H, W, seed=3, n_blobs=8):
@@ -100,7 +110,7 @@ def test_short_horizon_matches_oracle(cuda, shape, n):
     plan.close()
     ref = oracle.hio(M, mask, n, 1e-30, 0.9)
     assert iters == ref.iterations == n
-    assert _rel(out, ref.out) < 1e-4
+    _assert_close_to_oracle(out, ref.out, M, mask, n)
     np.testing.assert_allclose(errs[:n + 1], ref.errors[:n + 1], rtol=1e-4)
 
 
@@ -172,7 +182,7 @@ def test_device_buffers_and_seed(cuda):
     np.testing.assert_array_equal(out.cpu().numpy(), plan.execute_host(M, mask))
     other = plan.execute_host(M, mask, seed=7)
     plan.close()
-    assert _rel(other, oracle.hio(M, mask, 8, 1e-30, 0.9, seed=7).out) < 1e-4
+    _assert_close_to_oracle(other, oracle.hio(M, mask, 8, 1e-30, 0.9, seed=7).out, M, mask, 8, seed=7)
 
 
 def test_unsupported_size_and_null_arguments(cuda):
