@@ -40,8 +40,46 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b)
 {
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// Complex add and subtract as one packed two-lane FP32 instruction each
+// (add/sub.rn.f32x2 of sm_100): per lane the same IEEE round-to-nearest
+// operation as the scalar form, half the instructions.
+__device__ __forceinline__ unsigned long long f2pack(float2 a)
+{
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+    return r;
+}
+__device__ __forceinline__ float2 f2unpack(unsigned long long r)
+{
+    float2 a;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a.x), "=f"(a.y) : "l"(r));
+    return a;
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b)
+{
+    unsigned long long r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2pack(a)), "l"(f2pack(b)));
+    return f2unpack(r);
+}
+__device__ __forceinline__ float2 csub(float2 a, float2 b)
+{
+    unsigned long long r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2pack(a)), "l"(f2pack(b)));
+    return f2unpack(r);
+}
+// a + S*i*d and a - S*i*d: (a.x -+ S d.y, a.y +- S d.x), one packed fma with
+// exact +-1 factors each (a single rounding, as the scalar subtraction).
+template <int S>
+__device__ __forceinline__ void cadd_sub_si(float2 a, float2 d, float2 &plus, float2 &minus)
+{
+    const unsigned long long sw = f2pack(make_float2(d.y, d.x)), pa = f2pack(a);
+    const unsigned long long kp = f2pack(make_float2((float)-S, (float)S)), km = f2pack(make_float2((float)S, (float)-S));
+    unsigned long long rp, rm;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(rp) : "l"(sw), "l"(kp), "l"(pa));
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(rm) : "l"(sw), "l"(km), "l"(pa));
+    plus = f2unpack(rp);
+    minus = f2unpack(rm);
+}
 // multiply by S*i
 template <int S>
 __device__ __forceinline__ float2 mul_si(float2 a) { return S > 0 ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x); }
@@ -59,11 +97,10 @@ template <int S>
 __device__ __forceinline__ void dft4(float2 *v)
 {
     float2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
-    float2 a2 = cadd(v[1], v[3]), a3 = mul_si<S>(csub(v[1], v[3]));
+    float2 a2 = cadd(v[1], v[3]), d = csub(v[1], v[3]);
     v[0] = cadd(a0, a2);
     v[2] = csub(a0, a2);
-    v[1] = cadd(a1, a3);
-    v[3] = csub(a1, a3);
+    cadd_sub_si<S>(a1, d, v[1], v[3]);   // a1 +- S i d
 }
 
 template <int S>
@@ -76,14 +113,12 @@ __device__ __forceinline__ void dft8(float2 *v)
     dft4<S>(o);
     // w^1 = c*(1 + S i), w^2 = S i, w^3 = c*(-1 + S i)
     float2 o1 = make_float2(c * (o[1].x - S * o[1].y), c * (S * o[1].x + o[1].y));
-    float2 o2 = mul_si<S>(o[2]);
     float2 o3 = make_float2(c * (-o[3].x - S * o[3].y), c * (S * o[3].x - o[3].y));
     v[0] = cadd(e[0], o[0]);
     v[4] = csub(e[0], o[0]);
     v[1] = cadd(e[1], o1);
     v[5] = csub(e[1], o1);
-    v[2] = cadd(e[2], o2);
-    v[6] = csub(e[2], o2);
+    cadd_sub_si<S>(e[2], o[2], v[2], v[6]);   // e2 +- S i o2
     v[3] = cadd(e[3], o3);
     v[7] = csub(e[3], o3);
 }

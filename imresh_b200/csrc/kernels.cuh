@@ -182,14 +182,13 @@ __device__ __forceinline__ void hio_tile_done(const JobDev &J, int tile, double 
 
 // Per-element part of the fixed-support HIO row pass: error terms of g' and
 // out = Re(g') when this iteration is tested (or is the last).
-__device__ __forceinline__ void hio_track(const JobDev &J, size_t idx, float2 gp1, uint8_t m, double &tot,
-                                          double &cnt)
+__device__ __forceinline__ void hio_track(float *out, size_t idx, float2 gp1, uint8_t m, double &tot, double &cnt)
 {
     if (m) {
         tot += (double)m * (double)cnorm_ref(gp1);
         cnt += (double)m;
     }
-    J.out[idx] = gp1.x;
+    out[idx] = gp1.x;
 }
 
 template <int NT>
@@ -376,7 +375,7 @@ __device__ __forceinline__ void b_row_hio(const JobDev *jobs, const WorkItem wi)
             m = J.mask[idx];
         }
         if (FIX) {
-            if (track) hio_track(J, idx, gp1, m, tot, cnt);
+            if (track) hio_track(J.out, idx, gp1, m, tot, cnt);
             if (fin) continue;
         }
         const float2 gp = init_gprev ? gp1 : J.G[idx];
@@ -866,7 +865,7 @@ __device__ __forceinline__ void b_row_hio_r(const JobDev *jobs, const WorkItem w
             } else {
                 msk = J.mask[idx];
             }
-            if (FIX && track) hio_track(J, idx, gp1, msk, tot, cnt);
+            if (FIX && track) hio_track(J.out, idx, gp1, msk, tot, cnt);
             if (fin) continue;
             const float2 gp = init_gprev ? gp1 : J.G[idx];
             float2 g;
@@ -1059,6 +1058,7 @@ __global__ void __launch_bounds__(rrow_threads(N)) k_row_hio_p(const JobDev *job
         else tma_load_1d(st + 2 * XB, J.mask + (size_t)y0 * N, mb, &bars[s]);
     };
 
+    __shared__ int s_next[2];   // next item, found by thread 0 (double-buffered by iteration parity)
     if (threadIdx.x == 0) {
         mbar_init(&bars[0], 1);
         mbar_init(&bars[1], 1);
@@ -1071,15 +1071,31 @@ __global__ void __launch_bounds__(rrow_threads(N)) k_row_hio_p(const JobDev *job
     RegTw<N> rtw;
     if (item < n_items) rtw.load(jobs[item_at(L, item).job].prow.tw, l);
     for (int k = 0; item < n_items; ++k) {
-        const int nxt = next_live(item + gridDim.x);
         const int s = k & 1;
-        if (threadIdx.x == 0 && nxt < n_items) {
-            fence_proxy_async_smem();
-            issue(nxt, s ^ 1);
+        int nxt = n_items;
+        if (threadIdx.x == 0) {
+            nxt = next_live(item + gridDim.x);
+            s_next[s] = nxt;
+            if (nxt < n_items) {
+                fence_proxy_async_smem();
+                issue(nxt, s ^ 1);
+            }
         }
+        // this item's job fields, loaded before the wait so that their latency overlaps it
         const WorkItem wi = item_at(L, item);
         const JobDev &J = jobs[wi.job];
-        JobState *st = J.st;
+        JobState *const st = J.st;
+        float2 *const Xg = J.X;
+        float2 *const Gg = J.G;
+        uint8_t *const Mk = J.mask;
+        float *const outp = J.out;
+        const int rpc = J.rpc, H = J.H;
+        const float beta = J.beta;
+        const float thr = FIRST ? st->thr : 0.f;
+        const bool first_cycle = FIRST && st->hio_cycle == 0;
+        const int kit = FIX ? st->cycle : 0;
+        const bool fin = FIX && kit >= J.n_cycles;
+        const bool tested = FIX && (J.target > 0.f || fin);
         const bool landed = mbar_wait(&bars[s], (uint32_t)((k >> 1) & 1));
         if (__syncthreads_or(!landed)) {
             if (threadIdx.x == 0) {
@@ -1091,19 +1107,15 @@ __global__ void __launch_bounds__(rrow_threads(N)) k_row_hio_p(const JobDev *job
         unsigned char *stg = stages + s * STAGE;
         float2 *sX = reinterpret_cast<float2 *>(stg);
         const float2 *sG = reinterpret_cast<const float2 *>(stg + XB);
-        const int y = wi.tile * J.rpc + b;
-        const bool ok = b < J.rpc && y < J.H;
+        const int y = wi.tile * rpc + b;
+        const bool ok = b < rpc && y < H;
         const size_t base = (size_t)y * N;
         float2 v[V];
 #pragma unroll
         for (int m = 0; m < V; ++m) v[m] = sX[b * N + l + m * Q];
         reg_fft_1buf<N, RowSwz<N, NB>, +1>(v, sX, b, l, rtw);
-        const float beta = J.beta;
-        const float thr = st->thr;
-        const int kit = FIX ? st->cycle : 0;
-        const bool init_gprev = FIX ? kit == 0 : FIRST && st->hio_cycle == 0;
-        const bool fin = FIX && kit >= J.n_cycles;
-        const bool track = FIX && ok && (J.target > 0.f || fin);
+        const bool init_gprev = FIX ? kit == 0 : first_cycle;
+        const bool track = tested && ok;
         double tot = 0.0, cnt = 0.0;
 #pragma unroll
         for (int m = 0; m < V; ++m) {
@@ -1113,7 +1125,7 @@ __global__ void __launch_bounds__(rrow_threads(N)) k_row_hio_p(const JobDev *job
             if constexpr (FIRST) msk = reinterpret_cast<const float *>(stg + 2 * XB)[e] < thr ? 1 : 0;
             else msk = (stg + 2 * XB)[e];
             if constexpr (FIX) {
-                if (track) hio_track(J, base + l + m * Q, gp1, msk, tot, cnt);
+                if (track) hio_track(outp, base + l + m * Q, gp1, msk, tot, cnt);
             }
             const float2 gp = init_gprev ? gp1 : sG[e];
             float2 g;
@@ -1123,8 +1135,8 @@ __global__ void __launch_bounds__(rrow_threads(N)) k_row_hio_p(const JobDev *job
             else
                 g = gp1;
             if (ok && !fin) {
-                J.G[base + l + m * Q] = g;
-                if constexpr (FIRST) J.mask[base + l + m * Q] = msk;
+                Gg[base + l + m * Q] = g;
+                if constexpr (FIRST) Mk[base + l + m * Q] = msk;
             }
             v[m] = g;
         }
@@ -1132,13 +1144,13 @@ __global__ void __launch_bounds__(rrow_threads(N)) k_row_hio_p(const JobDev *job
             reg_fft_1buf<N, RowSwz<N, NB>, -1>(v, sX, b, l, rtw);
             if (ok) {
 #pragma unroll
-                for (int m = 0; m < V; ++m) J.X[base + l + m * Q] = v[m];
+                for (int m = 0; m < V; ++m) Xg[base + l + m * Q] = v[m];
             }
         }
         if constexpr (FIX) hio_tile_done<rrow_threads(N)>(J, wi.tile, tot, cnt);
         fence_proxy_async_smem();
-        __syncthreads();   // stage s is free for the copy issued next iteration
-        item = nxt;
+        __syncthreads();   // stage s is free for the copy issued next iteration; s_next[s] is visible
+        item = s_next[s];
     }
 }
 
@@ -1320,14 +1332,20 @@ k_col_p16(const JobDev *jobs, const WorkList *L)
     if (item < n_items) rtw.load(jobs[item_at(L, item).job].pcol.tw, l);
     __syncthreads();
     if (threadIdx.x == 0 && item < n_items) issue(item, 0);
+    __shared__ int s_next[2];   // next item, found by thread 0 (double-buffered by iteration parity)
     for (int k = 0; item < n_items; ++k) {
-        const int nxt = next_live(item + gridDim.x);
         const int s = k & 1;
+        int nxt = n_items;
+        if (threadIdx.x == 0) {
+            nxt = next_live(item + gridDim.x);
+            s_next[s] = nxt;
+        }
         const WorkItem wi = item_at(L, item);
         const JobDev &J = jobs[wi.job];
         const int W = J.W;
         const int x = wi.tile * NB + b;
         const bool ok = x < W;
+        const bool guard = J.mode == kModeShrinkWrap;
         float mod[V];
         if constexpr (!TM) {
 #pragma unroll
@@ -1352,7 +1370,6 @@ k_col_p16(const JobDev *jobs, const WorkList *L)
             fence_proxy_async_smem();
             issue(nxt, s ^ 1);
         }
-        const bool guard = J.mode == kModeShrinkWrap;
 #pragma unroll
         for (int m = 0; m < V; ++m) {
             if constexpr (TM) mod[m] = reinterpret_cast<const float *>(stg + XB)[(l + m * Q) * NB + b];
@@ -1373,7 +1390,7 @@ k_col_p16(const JobDev *jobs, const WorkList *L)
             for (int r0 = 0; r0 < N; r0 += BR) tma_store_2d(&J.tmX, x0, r0, sX + (size_t)r0 * NB);
             bulk_commit();
         }
-        item = nxt;
+        item = s_next[s];   // written before the barriers above
     }
     if (threadIdx.x == 0) bulk_wait0();
 }
