@@ -193,6 +193,23 @@ int imr_hio_plan_stats(imr_hio_plan *plan, void *stream, int *iterations, float 
 int imr_hio_plan_destroy(imr_hio_plan *plan);
 
 /* ------------------------------------------------------------------------
+ * Image files (host memory) behind the task queue's read-in / write-out
+ * callbacks (src/imresh/io/readInFuncs/readInFuncs.hpp:57-84,
+ * src/imresh/io/writeOutFuncs/writeOutFuncs.hpp:52-106) for formats that need
+ * no third-party library: NumPy .npy (float32 written; float32 or float64,
+ * 1-D or 2-D, C order read), text (one image row per line) and headerless
+ * float32.  W*H floats, width contiguous.  Readers allocate *data (release it
+ * with imr_free_image); failures return IMR_ERR_INVALID_VALUE with a message
+ * on stderr.
+ */
+int imr_write_npy(const char *path, const float *data, unsigned W, unsigned H);
+int imr_read_npy(const char *path, float **data, unsigned *W, unsigned *H);
+int imr_write_txt(const char *path, const float *data, unsigned W, unsigned H);
+int imr_read_txt(const char *path, float **data, unsigned *W, unsigned *H);
+int imr_write_raw(const char *path, const float *data, unsigned W, unsigned H);
+void imr_free_image(float *data);
+
+/* ------------------------------------------------------------------------
  * Reconstruction that allocates nothing -- no counterpart in the reference.
  * For callers that cannot call cudaMalloc (memory owned by a fixed arena or a
  * framework allocator, loops that must not take the driver's allocation

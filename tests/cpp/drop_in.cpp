@@ -20,6 +20,7 @@
 #include "algorithms/cuda/cudaVectorReduce.hpp"
 #include "libs/hybridInputOutput.hpp"
 #include "io/taskQueue.cu"
+#include "io/readInFuncs/readInFuncs.hpp"
 #include "io/writeOutFuncs/writeOutFuncs.hpp"
 #include "libs/diffractionIntensity.hpp"
 
@@ -124,6 +125,29 @@ int main()
     if (count != 1366.f || total != 5.f * count || !(err > 0) || mx != 4.f) {
         std::printf("reductions: count %g total %g err %g max %g\n", count, total, err, mx);
         return 1;
+    }
+    // file callbacks: a task result written with writeOutNpy / writeOutTxt and read back
+    {
+        const unsigned w = 5, h = 3;
+        float *img = new float[w * h];
+        for (unsigned i = 0; i < w * h; ++i) img[i] = 0.25f * i - 1.f;
+        const std::string npy = "drop_in_io_test.npy", txt = "drop_in_io_test.txt";
+        imresh::io::writeOutFuncs::writeOutNpy(img, w, h, npy);
+        imresh::io::writeOutFuncs::writeOutAndFreeTxt(img, w, h, txt);   // releases img
+        auto a = imresh::io::readInFuncs::readNpy(npy);
+        auto b = imresh::io::readInFuncs::readTxt(txt);
+        bool same = a.first && b.first && a.second.first == w && a.second.second == h &&
+                    b.second.first == w && b.second.second == h;
+        for (unsigned i = 0; same && i < w * h; ++i)
+            same = a.first[i] == 0.25f * i - 1.f && b.first[i] == a.first[i];
+        imresh::io::writeOutFuncs::justFree(a.first, w, h, npy);
+        imresh::io::writeOutFuncs::justFree(b.first, w, h, txt);
+        std::remove(npy.c_str());
+        std::remove(txt.c_str());
+        if (!same) {
+            std::printf("file callbacks: read-back mismatch\n");
+            return 1;
+        }
     }
     std::printf("OK\n");
     return 0;

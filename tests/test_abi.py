@@ -67,5 +67,8 @@ def test_reference_symbols_exported():
     for sym in ("imresh::algorithms::cuda::cudaShrinkWrap(", "imresh::io::taskQueueInit()",
                 "imresh::io::taskQueueDeinit()", "imresh::io::addTask(",
                 "imresh::io::writeOutFuncs::justFree(", "imresh::libs::diffractionIntensity(",
-                "imresh::libs::hybridInputOutput("):
+                "imresh::libs::hybridInputOutput(", "imresh::io::readInFuncs::readTxt(",
+                "imresh::io::readInFuncs::readNpy(", "imresh::io::writeOutFuncs::writeOutNpy(",
+                "imresh::io::writeOutFuncs::writeOutAndFreeNpy(", "imresh::io::writeOutFuncs::writeOutTxt(",
+                "imresh::io::writeOutFuncs::writeOutRaw("):
         assert sym in out, sym

@@ -110,6 +110,6 @@ def test_diffraction_intensity_matches_numpy(cuda):
 def test_reference_api_cpp_program_runs(cuda, tmp_path):
     from tests.cpp_build import build_drop_in
     exe = build_drop_in(str(tmp_path))
-    r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=300, cwd=str(tmp_path))
     assert r.returncode == 0, r.stdout + r.stderr
     assert "OK" in r.stdout
