@@ -287,6 +287,10 @@ def _engine_sigs(L):
     L.imr_engine_stats.argtypes = [vp, C.POINTER(CEngineInfo)]
     L.imr_engine_destroy.argtypes = [vp]
     L.imr_diffraction_intensity.argtypes = [vp, C.c_uint, C.c_uint, vp]
+    L.imr_engine_snapshot_size.argtypes = [vp, C.c_longlong, C.POINTER(C.c_size_t)]
+    L.imr_engine_checkpoint.argtypes = [vp, C.c_longlong, vp, C.c_size_t]
+    L.imr_engine_suspend.argtypes = [vp, C.c_longlong, vp, C.c_size_t]
+    L.imr_engine_resume.argtypes = [vp, vp, C.c_size_t, vp]
 
 
 class Engine:
@@ -333,6 +337,35 @@ class Engine:
             out.append(dict(tag=r.tag, width=r.width, height=r.height, cycles_done=r.cycles_done,
                             last_error=r.last_error, latency_ms=r.latency_ms, status=r.status,
                             out=o))
+        return out
+
+    def _snapshot(self, fn, tag: int) -> bytes:
+        n = C.c_size_t()
+        _check(lib().imr_engine_snapshot_size(self._h, tag, C.byref(n)), "imr_engine_snapshot_size")
+        buf = np.empty(n.value, np.uint8)
+        _check(getattr(lib(), fn)(self._h, tag, buf.ctypes.data, n.value), fn)
+        return buf.tobytes()
+
+    def checkpoint(self, tag: int) -> bytes:
+        """Saved state of the running reconstruction `tag` (it keeps running)."""
+        return self._snapshot("imr_engine_checkpoint", tag)
+
+    def suspend(self, tag: int) -> bytes:
+        """Saved state of the running reconstruction `tag`, which leaves the engine."""
+        snap = self._snapshot("imr_engine_suspend", tag)
+        self._keep.pop(tag, None)
+        return snap
+
+    def resume(self, snapshot: bytes, out: np.ndarray | None = None) -> np.ndarray:
+        """Queue a saved reconstruction; it continues where it was saved."""
+        buf = np.frombuffer(snapshot, np.uint8)
+        W, H = np.frombuffer(snapshot[8:16], np.uint32)
+        tag = int(np.frombuffer(snapshot[48:56], np.int64)[0])
+        if out is None:
+            out = np.empty((int(H), int(W)), np.float32)
+        _check(lib().imr_engine_resume(self._h, buf.ctypes.data, buf.size, out.ctypes.data),
+               "imr_engine_resume")
+        self._keep[tag] = (buf, out)
         return out
 
     def info(self) -> dict:

@@ -12,8 +12,10 @@
 // of different sizes therefore share every launch of their class; new
 // requests are admitted between steps as device memory frees up, finished
 // ones (stop test met or cycles exhausted, decided on the device) retire and
-// their results are copied out.
+// their results are copied out.  Between steps a reconstruction can be saved
+// to host memory and suspended, and resumed later in this or another engine.
 #include <cuda_runtime.h>
+#include <stdint.h>
 #include <string.h>
 
 #include <algorithm>
@@ -48,7 +50,29 @@ struct EJob {
     int cycles_done = 0;
     float last_error = 0.f;
     int status = IMR_SUCCESS;
+    std::vector<char> resume;   // snapshot to continue from (empty: a new request)
 };
+
+// Snapshot of one reconstruction between engine steps: the header, then
+// X, g_prev (complex64), the modulus (float32), the support mask (bytes)
+// and the per-cycle errors (float32), each W*H (errors: n_err) long.
+struct SnapHeader {
+    char magic[8];
+    uint32_t W, H;
+    imr_params p;
+    long long tag;
+    JobState st;
+    uint32_t n_err;
+    uint32_t pad;
+    uint64_t bytes;
+};
+constexpr char kSnapMagic[8] = {'I', 'M', 'R', 'S', 'N', 'A', 'P', '1'};
+
+static size_t snap_bytes(unsigned W, unsigned H, unsigned n_err)
+{
+    const size_t N = (size_t)W * H;
+    return sizeof(SnapHeader) + N * 8 * 2 + N * 4 + N + (size_t)n_err * 4;
+}
 
 // kernels + list slice of one launch group
 struct Group {
@@ -143,10 +167,26 @@ static int admit(imr_engine *E, std::vector<EJob *> &fresh)
         job_bind(j->J, j->S, j->arena, E->dst + j->slot);
         int rc = job_upload(j->J, j->S, j->arena, E->dj + j->slot, E->s);
         if (rc) return rc;
-        CKE(cudaMemsetAsync(E->dst + j->slot, 0, sizeof(JobState), E->s));
-        CKE(cudaMemcpyAsync((void *)j->J.M, j->h_in, (size_t)j->W * j->H * 4, cudaMemcpyHostToDevice, E->s));
+        if (j->resume.empty()) {
+            CKE(cudaMemsetAsync(E->dst + j->slot, 0, sizeof(JobState), E->s));
+            CKE(cudaMemcpyAsync((void *)j->J.M, j->h_in, (size_t)j->W * j->H * 4, cudaMemcpyHostToDevice, E->s));
+            fresh.push_back(j);
+        } else {   // continue a suspended reconstruction where it stopped
+            const SnapHeader *h = (const SnapHeader *)j->resume.data();
+            const size_t N = (size_t)j->W * j->H;
+            const char *d = j->resume.data() + sizeof(SnapHeader);
+            // on the engine's stream, after job_upload's clearing of the mask and
+            // errors; a copy from pageable memory has staged its source on return
+            CKE(cudaMemcpyAsync(E->dst + j->slot, &h->st, sizeof(JobState), cudaMemcpyHostToDevice, E->s));
+            CKE(cudaMemcpyAsync(j->J.X, d, N * 8, cudaMemcpyHostToDevice, E->s));
+            CKE(cudaMemcpyAsync(j->J.G, d + N * 8, N * 8, cudaMemcpyHostToDevice, E->s));
+            CKE(cudaMemcpyAsync((void *)j->J.M, d + N * 16, N * 4, cudaMemcpyHostToDevice, E->s));
+            CKE(cudaMemcpyAsync(j->J.mask, d + N * 20, N, cudaMemcpyHostToDevice, E->s));
+            CKE(cudaMemcpyAsync(j->J.errors, d + N * 21, (size_t)h->n_err * 4, cudaMemcpyHostToDevice, E->s));
+            CKE(cudaStreamSynchronize(E->s));
+            std::vector<char>().swap(j->resume);
+        }
         E->active.push_back(j);
-        fresh.push_back(j);
     }
     return IMR_SUCCESS;
 }
@@ -405,6 +445,91 @@ int imr_engine_run(imr_engine *E)
         int rc = imr_engine_step(E);
         if (rc) return rc;
     }
+    return IMR_SUCCESS;
+}
+
+static EJob *find_active(imr_engine *E, long long tag)
+{
+    for (EJob *j : E->active)
+        if (j->tag == tag) return j;
+    return nullptr;
+}
+
+int imr_engine_snapshot_size(imr_engine *E, long long tag, size_t *bytes)
+{
+    if (!E || !bytes) return IMR_ERR_INVALID_VALUE;
+    EJob *j = find_active(E, tag);
+    if (!j) return IMR_ERR_INVALID_VALUE;
+    *bytes = snap_bytes(j->W, j->H, (unsigned)j->J.n_cycles + 1);
+    return IMR_SUCCESS;
+}
+
+int imr_engine_checkpoint(imr_engine *E, long long tag, void *h_buf, size_t cap)
+{
+    if (!E || !h_buf) return IMR_ERR_INVALID_VALUE;
+    EJob *j = find_active(E, tag);
+    if (!j) return IMR_ERR_INVALID_VALUE;
+    const unsigned n_err = (unsigned)j->J.n_cycles + 1;
+    const size_t bytes = snap_bytes(j->W, j->H, n_err), N = (size_t)j->W * j->H;
+    if (cap < bytes) return IMR_ERR_INVALID_VALUE;
+    CKE(cudaStreamSynchronize(E->s));   // between steps the device state is at rest
+    SnapHeader h;
+    memset(&h, 0, sizeof(h));
+    memcpy(h.magic, kSnapMagic, 8);
+    h.W = j->W;
+    h.H = j->H;
+    h.p = j->p;
+    h.tag = j->tag;
+    h.n_err = n_err;
+    h.bytes = bytes;
+    CKE(cudaMemcpy(&h.st, E->dst + j->slot, sizeof(JobState), cudaMemcpyDeviceToHost));
+    char *d = (char *)h_buf;
+    memcpy(d, &h, sizeof(h));
+    d += sizeof(h);
+    CKE(cudaMemcpy(d, j->J.X, N * 8, cudaMemcpyDeviceToHost));
+    CKE(cudaMemcpy(d + N * 8, j->J.G, N * 8, cudaMemcpyDeviceToHost));
+    CKE(cudaMemcpy(d + N * 16, j->J.M, N * 4, cudaMemcpyDeviceToHost));
+    CKE(cudaMemcpy(d + N * 20, j->J.mask, N, cudaMemcpyDeviceToHost));
+    CKE(cudaMemcpy(d + N * 21, j->J.errors, (size_t)n_err * 4, cudaMemcpyDeviceToHost));
+    return IMR_SUCCESS;
+}
+
+int imr_engine_suspend(imr_engine *E, long long tag, void *h_buf, size_t cap)
+{
+    int rc = imr_engine_checkpoint(E, tag, h_buf, cap);
+    if (rc) return rc;
+    EJob *j = find_active(E, tag);
+    E->active.erase(std::find(E->active.begin(), E->active.end(), j));
+    CKE(cudaFreeAsync(j->arena, E->s));
+    CKE(cudaStreamSynchronize(E->s));
+    E->used -= j->S.bytes;
+    E->free_slots.push_back(j->slot);
+    delete j;
+    return IMR_SUCCESS;
+}
+
+int imr_engine_resume(imr_engine *E, const void *h_buf, size_t bytes, float *h_out)
+{
+    if (!E || !h_buf || !h_out || bytes < sizeof(SnapHeader)) return IMR_ERR_INVALID_VALUE;
+    SnapHeader h;
+    memcpy(&h, h_buf, sizeof(h));
+    if (memcmp(h.magic, kSnapMagic, 8) != 0 || h.W == 0 || h.H == 0 || h.bytes != bytes ||
+        bytes != snap_bytes(h.W, h.H, h.n_err) || h.n_err != h.p.nCycles + 1)
+        return IMR_ERR_INVALID_VALUE;
+    EJob *j = new EJob();
+    j->W = h.W;
+    j->H = h.H;
+    j->p = h.p;
+    int rc = job_prepare(h.W, h.H, j->p, j->J, j->S);
+    if (rc) {
+        delete j;
+        return rc;
+    }
+    j->resume.assign((const char *)h_buf, (const char *)h_buf + bytes);
+    j->h_out = h_out;
+    j->tag = h.tag;
+    j->t_submit = now_ms();
+    E->pending.push_back(j);
     return IMR_SUCCESS;
 }
 

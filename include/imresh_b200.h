@@ -269,6 +269,20 @@ int imr_engine_run(imr_engine *engine);
 /* Finished reconstructions since the last poll (up to max_results). */
 int imr_engine_poll(imr_engine *engine, imr_result *results, int max_results, int *n_results);
 int imr_engine_stats(imr_engine *engine, imr_engine_info *info);
+/* Suspend / resume of one reconstruction (for preemption and restart).  Between
+ * steps, a running reconstruction (`tag` of an active request) is saved into a
+ * HOST buffer of imr_engine_snapshot_size bytes: its iterate, g_prev, modulus,
+ * support mask, per-cycle errors and device-side cycle state.  checkpoint
+ * leaves it running; suspend also removes it from the engine and releases its
+ * device memory (no result is reported for it).  resume queues the saved
+ * reconstruction into this or another engine; it continues from the saved
+ * cycle, bit-identical to an uninterrupted run, and its result goes to h_out
+ * (W*H floats) under the saved tag.  Synchronous.  No counterpart in the
+ * reference (its tasks cannot be interrupted). */
+int imr_engine_snapshot_size(imr_engine *engine, long long tag, size_t *bytes);
+int imr_engine_checkpoint(imr_engine *engine, long long tag, void *h_buf, size_t capacity);
+int imr_engine_suspend(imr_engine *engine, long long tag, void *h_buf, size_t capacity);
+int imr_engine_resume(imr_engine *engine, const void *h_buf, size_t bytes, float *h_out);
 int imr_engine_destroy(imr_engine *engine);
 
 #ifdef __cplusplus

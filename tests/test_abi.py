@@ -51,6 +51,8 @@ def test_invalid_arguments_rejected_without_device():
     h = C.c_void_p()
     assert L.imr_plan_create(C.byref(h), 0, 4, None) == 1
     assert L.imr_plan_destroy(None) == 0
+    assert L.imr_engine_resume(None, buf.ctypes.data, 64, buf.ctypes.data) == 1
+    assert L.imr_engine_checkpoint(None, 0, buf.ctypes.data, 64) == 1
 
 
 def test_cpp_drop_in_compiles_and_links(tmp_path):

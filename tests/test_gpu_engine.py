@@ -113,3 +113,67 @@ def test_reference_api_cpp_program_runs(cuda, tmp_path):
     r = subprocess.run([exe], capture_output=True, text=True, timeout=300, cwd=str(tmp_path))
     assert r.returncode == 0, r.stdout + r.stderr
     assert "OK" in r.stdout
+
+
+def test_suspend_resume_is_bit_identical(cuda):
+    """A reconstruction saved between steps, removed, and resumed in another
+    engine finishes exactly as it would have uninterrupted; the engine it left
+    finishes its other work unchanged."""
+    p = imr.Params(6, imr.FLT_MIN, 0.9, 0.04, 0.2, 3.0, 0.01, 5)
+    Ma, _ = data.make_modulus(data.BlobSpec(256, 192, 20, 30.0, (1.5, 2.5), (0.5, 1.0), 1e8), 7, 0)
+    Mb, _ = data.make_modulus(data.BlobSpec(128, 128, 12, 20.0, (1.5, 2.5), (0.5, 1.0), None), 7, 1)
+    ref = imr.Engine()
+    ra, rb = ref.submit(Ma, p, tag=1), ref.submit(Mb, p, tag=2)
+    ref.run()
+    cyc = {r["tag"]: r["cycles_done"] for r in ref.poll()}
+    ref.close()
+
+    E = imr.Engine()
+    E.submit(Ma, p, tag=1)
+    ob = E.submit(Mb, p, tag=2)
+    E.step()
+    E.step()
+    snap = E.suspend(1)
+    assert E.info()["active"] == 1
+    E.step()
+    E2 = imr.Engine()
+    oa = E2.resume(snap)
+    E2.run()
+    E.run()
+    res2 = E2.poll()
+    assert [r["tag"] for r in res2] == [1] and res2[0]["cycles_done"] == cyc[1]
+    np.testing.assert_array_equal(oa, ra)
+    np.testing.assert_array_equal(ob, rb)
+    assert [r["tag"] for r in E.poll()] == [2]
+    E.close()
+    E2.close()
+
+
+def test_checkpoint_keeps_running_and_restarts_identically(cuda):
+    p = imr.Params(5, imr.FLT_MIN, 0.9, 0.04, 0.2, 3.0, 0.01, 4)
+    M, _ = data.make_modulus(data.BlobSpec(192, 256, 16, 30.0, (1.5, 2.5), (0.5, 1.0), 1e8), 9, 0)
+    ref = imr.Engine()
+    r = ref.submit(M, p, tag=5)
+    ref.run()
+    ref.close()
+    E = imr.Engine()
+    o = E.submit(M, p, tag=5)
+    E.step()
+    cp = E.checkpoint(5)
+    E.run()
+    np.testing.assert_array_equal(o, r)
+    E2 = imr.Engine()
+    o2 = E2.resume(cp)
+    E2.run()
+    np.testing.assert_array_equal(o2, r)
+    E.close()
+    E2.close()
+
+
+def test_snapshot_rejects_unknown_tags_and_bad_buffers(cuda):
+    E = imr.Engine()
+    with pytest.raises(imr.ImrError):
+        E.checkpoint(99)
+    with pytest.raises(imr.ImrError):
+        E.resume(b"IMRSNAP1" + bytes(200))
+    E.close()
