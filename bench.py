@@ -120,12 +120,15 @@ def run_batched(n_jobs: int = 512, plain_sample: int = 64):
     specs = data.cfg2_specs(n_jobs, seed=2)
     inputs = [data.make_modulus(sp, seed=2, index=i)[0] for i, sp in enumerate(specs)]
     prm = imr.Params(64, imr.FLT_MIN, 0.9, 0.04, 0.2, 3.0, 0.01, 20)
-    # warm-up: one small job of every shape class through the engine
+    # warm-up: one short job of every shape in the batch through the engine
     eng = imr.Engine()
-    for i, M in enumerate(inputs[:8]):
-        eng.submit(M, imr.Params(1, imr.FLT_MIN, 0.9, 0.04, 0.2, 3.0, 0.01, 1), tag=i)
+    first = {}
+    for i, M in enumerate(inputs):
+        first.setdefault(M.shape, i)
+    for i in first.values():
+        eng.submit(inputs[i], imr.Params(1, imr.FLT_MIN, 0.9, 0.04, 0.2, 3.0, 0.01, 1), tag=i)
     eng.run()
-    eng.poll()
+    eng.poll(len(first))
     t0 = time.perf_counter()
     for i, M in enumerate(inputs):
         eng.submit(M, prm, tag=i)

@@ -93,6 +93,7 @@ using namespace imr;
 struct imr_engine {
     int dev = 0;
     cudaStream_t s = nullptr;
+    cudaMemPool_t pool = nullptr;   // the engine's own pool: freed arenas stay cached for new admissions
     size_t budget = 0, used = 0, peak = 0;
     int max_slots = 0;
     JobDev *dj = nullptr;           // [max_slots]
@@ -154,7 +155,7 @@ static int admit(imr_engine *E, std::vector<EJob *> &fresh)
         E->pending.pop_front();
         j->slot = E->free_slots.back();
         E->free_slots.pop_back();
-        cudaError_t e = cudaMallocAsync((void **)&j->arena, j->S.bytes, E->s);
+        cudaError_t e = cudaMallocFromPoolAsync((void **)&j->arena, j->S.bytes, E->pool, E->s);
         if (e != cudaSuccess) {   // allocation failed: back to the queue, retry later
             E->free_slots.push_back(j->slot);
             j->slot = -1;
@@ -278,8 +279,13 @@ static int launch_step(imr_engine *E, const std::vector<EJob *> &fresh)
     }
     // --- one shrink-wrap cycle of every live job
     for (auto &g : rowg) {
-        g.rk.finish<<<loop_grid(E, (int)g.items.size()), g.rk.threads, g.smem_fin, s>>>(E->dj, L + g.list_base,
-                                                                                     nullptr);
+        if (g.pipelined) {
+            if ((rc = launch_finish(g.rk, (int)g.items.size(), g.smem_fin, s, E->dj, L + g.list_base, nullptr)))
+                return rc;
+        } else {
+            g.rk.finish<<<loop_grid(E, (int)g.items.size()), g.rk.threads, g.smem_fin, s>>>(E->dj, L + g.list_base,
+                                                                                         nullptr);
+        }
         ++E->launches;
     }
     if (!vb.empty()) {
@@ -363,6 +369,24 @@ int imr_engine_create(imr_engine **out, size_t device_bytes, int max_jobs, void 
     cudaGetDevice(&E->dev);
     cudaDeviceGetAttribute(&E->sms, cudaDevAttrMultiProcessorCount, E->dev);
     E->s = (cudaStream_t)stream;
+    {   // a pool of its own that keeps freed memory (release threshold: never), so
+        // admitting a request after another retired does not go back to the driver
+        cudaMemPoolProps pp;
+        memset(&pp, 0, sizeof(pp));
+        pp.allocType = cudaMemAllocationTypePinned;
+        pp.handleTypes = cudaMemHandleTypeNone;
+        pp.location.type = cudaMemLocationTypeDevice;
+        pp.location.id = E->dev;
+        cudaError_t pe = cudaMemPoolCreate(&E->pool, &pp);
+        uint64_t keep = UINT64_MAX;
+        if (pe == cudaSuccess) pe = cudaMemPoolSetAttribute(E->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (pe != cudaSuccess) {
+            set_error("engine memory pool", pe);
+            if (E->pool) cudaMemPoolDestroy(E->pool);
+            delete E;
+            return IMR_ERR_CUDA;
+        }
+    }
     if (device_bytes == 0) {
         size_t fr = 0, tot = 0;
         cudaMemGetInfo(&fr, &tot);
@@ -564,6 +588,10 @@ int imr_engine_destroy(imr_engine *E)
     if (E->h_items) cudaFreeHost(E->h_items);
     if (E->d_lists) cudaFree(E->d_lists);
     if (E->h_lists) cudaFreeHost(E->h_lists);
+    if (E->pool) {
+        cudaStreamSynchronize(E->s);
+        cudaMemPoolDestroy(E->pool);
+    }
     delete E;
     return IMR_SUCCESS;
 }

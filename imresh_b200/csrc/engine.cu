@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <map>
 #include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "imresh_b200.h"
@@ -223,6 +224,8 @@ static RowKernels row_set()
                        prow_smem<true, N>(), prow_smem<false, N>(), 0};
         k.hio_fix = k_row_hio_r<false, N, true>;
         k.p_hio_fix = k_row_hio_p<false, N, true>;
+        k.p_finish = k_row_finish_p<N>;
+        k.p_smem_fin = pfin_smem<N>();
     } else if constexpr (N >= 8 && is_pow2(N)) {
         k = RowKernels{k_row_hio_r<true, N>, k_row_hio_r<false, N>, k_row_finish_r<N>,
                        k_fft_rows_r<-1, N>, k_fft_rows_r<+1, N>, rrow_nb(N), rrow_threads(N),
@@ -234,6 +237,8 @@ static RowKernels row_set()
                        k_row_hio_p<false, N>, prow_smem<true, N>(), prow_smem<false, N>(), 0};
         k.hio_fix = k_row_hio<false, N, true>;
         k.p_hio_fix = k_row_hio_p<false, N, true>;
+        k.p_finish = k_row_finish_p<N>;
+        k.p_smem_fin = pfin_smem<N>();
     } else {
         k = RowKernels{k_row_hio<true, N>, k_row_hio<false, N>, k_row_finish<N>, k_fft_rows<-1, N>,
                        k_fft_rows<+1, N>, row_nb(N), row_threads(N), 0, nullptr, nullptr, 0, 0,
@@ -266,16 +271,60 @@ static ColKernels col_set()
                           col_threads(N), 0, nullptr, 0, 0, 0, 0, N < 0 ? -N : 0};
 }
 
+// Resident CTAs per SM of a kernel at a launch shape, asked of the occupancy
+// calculator once per (device, kernel, shape): the engine launches hundreds
+// of persistent passes per step.
+struct OccKey {
+    int dev;
+    const void *k;
+    int threads, smem;
+    bool operator<(const OccKey &o) const
+    {
+        return std::tie(dev, k, threads, smem) < std::tie(o.dev, o.k, o.threads, o.smem);
+    }
+};
+static std::mutex g_occ_mu;
+static std::map<OccKey, std::pair<int, int>> g_occ;   // -> (CTAs per SM, SMs)
+
 int persistent_grid(const void *kernel, int threads, int smem, int items)
 {
-    int dev = 0, sms = 148, per_sm = 1;
+    int dev = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess ||
-        per_sm < 1)
-        per_sm = 1;
-    long g = (long)per_sm * sms;
+    const OccKey key{dev, kernel, threads, smem};
+    std::pair<int, int> occ;
+    {
+        std::lock_guard<std::mutex> lk(g_occ_mu);
+        auto it = g_occ.find(key);
+        if (it != g_occ.end()) {
+            occ = it->second;
+        } else {
+            int sms = 148, per_sm = 1;
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess ||
+                per_sm < 1)
+                per_sm = 1;
+            occ = {per_sm, sms};
+            g_occ[key] = occ;
+        }
+    }
+    const long g = (long)occ.first * occ.second;
     return (int)(g < items ? g : items);
+}
+
+int launch_finish(const RowKernels &rk, int items, size_t smem_fin, cudaStream_t s, const JobDev *dj,
+                  const WorkList *L, float2 *dbg)
+{
+    if (rk.p_finish)
+        rk.p_finish<<<persistent_grid((const void *)rk.p_finish, rk.threads, rk.p_smem_fin, items), rk.threads,
+                      rk.p_smem_fin, s>>>(dj, L, dbg);
+    else
+        rk.finish<<<items, rk.threads, smem_fin, s>>>(dj, L, dbg);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error("finish launch", e);
+        return IMR_ERR_CUDA;
+    }
+    return IMR_SUCCESS;
 }
 
 static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
@@ -398,6 +447,7 @@ int ensure_kernel_attributes()
         if (e == cudaSuccess && r.p_hio_first) e = allow_smem(r.p_hio_first);
         if (e == cudaSuccess) e = allow_smem(r.hio_fix);
         if (e == cudaSuccess && r.p_hio_fix) e = allow_smem(r.p_hio_fix);
+        if (e == cudaSuccess && r.p_finish) e = allow_smem(r.p_finish);
         if (e == cudaSuccess && c.p_col) e = allow_smem(c.p_col);
     }
     if (e == cudaSuccess) e = allow_smem(k_hblur);
@@ -497,7 +547,8 @@ static int plan_launch_cycle(imr_plan *P, cudaStream_t s)
     const JobDev &J = P->hj;
     const RowKernels &rk = P->rk;
     const ColKernels &ck = P->ck;
-    rk.finish<<<J.n_row_tiles, rk.threads, P->smem_fin, s>>>(P->dj, P->Lrow, P->dbg_gprime);
+    int rc = launch_finish(rk, J.n_row_tiles, P->smem_fin, s, P->dj, P->Lrow, P->dbg_gprime);
+    if (rc) return rc;
     k_vblur<<<J.n_vb_tiles, kVbThreads, 0, s>>>(P->dj, P->Lvb);
     for (int i = 0; i < J.n_hio; ++i) {
         if (P->p_rows) {
@@ -772,7 +823,7 @@ int imr_plan_execute(imr_plan *P, const float *d_modulus, float *d_out, void *st
     P->ck.init<<<J.n_col_tiles, P->ck.threads, P->smem_col, s>>>(P->dj, P->Lcol);
     CK(cudaGetLastError());
     for (int c = 0; c < J.n_cycles; ++c) CK(cudaGraphLaunch(P->gexec, s));
-    P->rk.finish<<<J.n_row_tiles, P->rk.threads, P->smem_fin, s>>>(P->dj, P->Lrow, P->dbg_gprime);
+    if (int rc = launch_finish(P->rk, J.n_row_tiles, P->smem_fin, s, P->dj, P->Lrow, P->dbg_gprime)) return rc;
     k_vblur<<<J.n_vb_tiles, kVbThreads, 0, s>>>(P->dj, P->Lvb);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(d_out, J.out, N * 4, cudaMemcpyDeviceToDevice, s));
@@ -790,7 +841,7 @@ int imr_plan_execute_host(imr_plan *P, const float *h_modulus, float *h_out, voi
     P->ck.init<<<J.n_col_tiles, P->ck.threads, P->smem_col, s>>>(P->dj, P->Lcol);
     CK(cudaGetLastError());
     for (int c = 0; c < J.n_cycles; ++c) CK(cudaGraphLaunch(P->gexec, s));
-    P->rk.finish<<<J.n_row_tiles, P->rk.threads, P->smem_fin, s>>>(P->dj, P->Lrow, P->dbg_gprime);
+    if (int rc = launch_finish(P->rk, J.n_row_tiles, P->smem_fin, s, P->dj, P->Lrow, P->dbg_gprime)) return rc;
     k_vblur<<<J.n_vb_tiles, kVbThreads, 0, s>>>(P->dj, P->Lvb);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(h_out, J.out, N * 4, cudaMemcpyDeviceToHost, s));

@@ -34,7 +34,7 @@ constexpr int kRowVpt = 8;          // complex values per thread per pass (rows,
 constexpr int kColThreads = 256;
 constexpr int kColVpt = 8;          // complex values per thread per pass (columns, runtime length)
 constexpr int kVbTileX = 32;
-constexpr int kVbTileY = 64;
+constexpr int kVbTileY = 128;
 constexpr int kVbThreads = 256;
 
 struct JobState {

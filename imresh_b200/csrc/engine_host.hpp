@@ -40,6 +40,9 @@ struct RowKernels {
     // and, where the length has one, the pipelined kernel (shared memory p_smem)
     void (*hio_fix)(const JobDev *, const WorkList *);
     void (*p_hio_fix)(const JobDev *, const WorkList *);
+    // pipelined once-per-cycle pass (g', out, error sums, row blur) or null
+    void (*p_finish)(const JobDev *, const WorkList *, float2 *);
+    int p_smem_fin;
 };
 // Kernels and launch shape of the column passes for one column length.
 struct ColKernels {
@@ -65,6 +68,10 @@ int fft_passes(float2 *d, int W, int H, int sign, int axes, const FftPlanDev &pr
                cudaStream_t s);
 // Persistent grid size for a pipelined kernel (CTAs per SM x SMs, <= items).
 int persistent_grid(const void *kernel, int threads, int smem, int items);
+// Launch the once-per-cycle row pass over `items` row tiles: the pipelined
+// persistent kernel where the row length has one, else one CTA per tile.
+int launch_finish(const RowKernels &rk, int items, size_t smem_fin, cudaStream_t s, const JobDev *dj,
+                  const WorkList *L, float2 *dbg);
 // 2D tensor map over a row-major [H][W] array of `elem`-byte elements with a
 // (box_w, box_h) box; returns false when the shape cannot be described.
 bool encode_tensor_map(CUtensorMap *map, const void *base, int W, int H, int elem, int box_w, int box_h);

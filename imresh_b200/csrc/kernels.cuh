@@ -238,16 +238,26 @@ __device__ __forceinline__ float vblur_tile(const float *src, float *dst, int W,
         tile[r * kVbTileX + tx] = x < W ? src[(size_t)ys * W + x] : 0.f;
     }
     __syncthreads();
+    // RPT outputs per thread, accumulated side by side (independent chains);
+    // each output still sums its taps in order k = 0..K-1
+    constexpr int RS = kVbThreads / kVbTileX, RPT = kVbTileY / RS;
+    float sum[RPT];
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) sum[j] = 0.f;
+    for (int k = 0; k < K; ++k) {
+        const float wk = w[k];
+#pragma unroll
+        for (int j = 0; j < RPT; ++j) sum[j] = __fadd_rn(sum[j], __fmul_rn(tile[(ty + j * RS + k) * kVbTileX + tx], wk));
+    }
     float mx = 0.f;
     if (x < W) {
-        for (int r = ty; r < kVbTileY; r += kVbThreads / kVbTileX) {
-            const int y = y0 + r;
-            if (y >= H) break;
-            float sum = 0.f;
-            for (int k = 0; k < K; ++k)
-                sum = __fadd_rn(sum, __fmul_rn(tile[(r + k) * kVbTileX + tx], w[k]));
-            dst[(size_t)y * W + x] = sum;
-            mx = fmaxf(mx, sum);
+#pragma unroll
+        for (int j = 0; j < RPT; ++j) {
+            const int y = y0 + ty + j * RS;
+            if (y < H) {
+                dst[(size_t)y * W + x] = sum[j];
+                mx = fmaxf(mx, sum[j]);
+            }
         }
     }
     return mx;
@@ -1148,6 +1158,132 @@ __global__ void __launch_bounds__(rrow_threads(N)) k_row_hio_p(const JobDev *job
             }
         }
         if constexpr (FIX) hio_tile_done<rrow_threads(N)>(J, wi.tile, tot, cnt);
+        fence_proxy_async_smem();
+        __syncthreads();   // stage s is free for the copy issued next iteration; s_next[s] is visible
+        item = s_next[s];
+    }
+}
+
+// ---- once per cycle, pipelined ----------------------------------------------
+// The work of b_row_finish_r on the persistent, TMA-fed skeleton of the row
+// pass: inverse row FFT -> g'; out = Re(g'); error sums of |g'| against the
+// previous cycle's mask; |g'| blurred along the row -> hb.  Stage: X rows and
+// mask rows; the X region holds the row norms for the blur once the FFT is
+// done with it.
+template <int N>
+__host__ __device__ constexpr int pfin_stage_bytes() { return round128(rrow_nb(N) * N * 8 + round16(rrow_nb(N) * N)); }
+template <int N>
+__host__ __device__ constexpr int pfin_smem() { return 128 + 2 * pfin_stage_bytes<N>(); }
+
+template <int N>
+__global__ void __launch_bounds__(rrow_threads(N)) k_row_finish_p(const JobDev *jobs, const WorkList *L, float2 *dbg_gprime)
+{
+    extern __shared__ __align__(128) unsigned char sbuf[];
+    constexpr int NB = rrow_nb(N), V = reg_v(N), Q = N / V, T = rrow_threads(N);
+    constexpr int XB = NB * N * 8;
+    constexpr int STAGE = pfin_stage_bytes<N>();
+    __shared__ float wsm[kTapStride];
+    __shared__ double red[2 * T / 32 > 2 ? 2 * T / 32 : 2];
+    __shared__ int s_next[2];
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sbuf);
+    unsigned char *stages = sbuf + 128;
+    const int b = threadIdx.x / Q, l = threadIdx.x % Q;
+    const int n_items = L->n;
+
+    auto next_live = [&](int it) {
+        while (it < n_items && !job_live(jobs, L, it)) it += gridDim.x;
+        return it;
+    };
+    auto issue = [&](int item, int s) {   // one thread
+        const WorkItem wi = item_at(L, item);
+        const JobDev &J = jobs[wi.job];
+        const int y0 = wi.tile * J.rpc;
+        const int nr = min(J.rpc, J.H - y0);
+        const uint32_t xb = (uint32_t)(nr * N * 8), mb = (uint32_t)round16(nr * N);
+        unsigned char *st = stages + s * STAGE;
+        mbar_arrive_expect_tx(&bars[s], xb + mb);
+        tma_load_1d(st, J.X + (size_t)y0 * N, xb, &bars[s]);
+        tma_load_1d(st + XB, J.mask + (size_t)y0 * N, mb, &bars[s]);
+    };
+
+    if (threadIdx.x == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    int item = next_live(blockIdx.x);
+    if (threadIdx.x == 0 && item < n_items) issue(item, 0);
+    RegTw<N> rtw;
+    if (item < n_items) rtw.load(jobs[item_at(L, item).job].prow.tw, l);
+    for (int k = 0; item < n_items; ++k) {
+        const int s = k & 1;
+        int nxt = n_items;
+        if (threadIdx.x == 0) {
+            nxt = next_live(item + gridDim.x);
+            s_next[s] = nxt;
+            if (nxt < n_items) {
+                fence_proxy_async_smem();
+                issue(nxt, s ^ 1);
+            }
+        }
+        const WorkItem wi = item_at(L, item);
+        const JobDev &J = jobs[wi.job];
+        JobState *const st = J.st;
+        float *const outp = J.out;
+        float *const hbp = J.hb;
+        const int rpc = J.rpc, H = J.H;
+        const int c = st->cycle;
+        const int K = J.ntaps[c];
+        if (threadIdx.x < kTapStride) wsm[threadIdx.x] = J.weights[(size_t)c * kTapStride + threadIdx.x];
+        if (wi.tile == 0 && threadIdx.x == 0) st->max_bits = 0u;
+        const bool landed = mbar_wait(&bars[s], (uint32_t)((k >> 1) & 1));
+        if (__syncthreads_or(!landed)) {
+            if (threadIdx.x == 0) {
+                atomicExch(&st->err, 1);
+                if (nxt < n_items) mbar_wait(&bars[s ^ 1], (uint32_t)(((k + 1) >> 1) & 1));
+            }
+            return;
+        }
+        unsigned char *stg = stages + s * STAGE;
+        float2 *sX = reinterpret_cast<float2 *>(stg);
+        const uint8_t *sM = stg + XB;
+        const int y = wi.tile * rpc + b;
+        const bool ok = b < rpc && y < H;
+        const size_t base = (size_t)y * N;
+        float2 v[V];
+#pragma unroll
+        for (int m = 0; m < V; ++m) v[m] = sX[b * N + l + m * Q];
+        reg_fft_1buf<N, RowSwz<N, NB>, +1>(v, sX, b, l, rtw);
+        __syncthreads();   // the FFT's last reads of the X region are done: it now holds the norms
+        float *nrow = reinterpret_cast<float *>(sX) + b * N;
+        double tot = 0.0, cnt = 0.0;
+#pragma unroll
+        for (int m = 0; m < V; ++m) {
+            const int e = l + m * Q;
+            const float nv = cnorm_ref(v[m]);
+            nrow[e] = nv;
+            if (ok) {
+                outp[base + e] = v[m].x;
+                if (dbg_gprime) dbg_gprime[base + e] = v[m];
+                if (c > 0 && sM[b * N + e]) {
+                    tot += (double)nv;
+                    cnt += 1.0;
+                }
+            }
+        }
+        block_sum2<T>(tot, cnt, red);   // includes barriers: nrow complete after it
+        if (threadIdx.x == 0) {
+            J.err_part[2 * wi.tile] = tot;
+            J.err_part[2 * wi.tile + 1] = cnt;
+        }
+        if (ok) {
+#pragma unroll
+            for (int m = 0; m < V; ++m) {
+                const int e = l + m * Q;
+                hbp[base + e] = hblur_at(nrow, N, e, wsm, K);
+            }
+        }
         fence_proxy_async_smem();
         __syncthreads();   // stage s is free for the copy issued next iteration; s_next[s] is visible
         item = s_next[s];

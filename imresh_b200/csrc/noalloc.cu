@@ -232,7 +232,7 @@ extern "C" int imr_shrink_wrap_noalloc(const float *d_modulus, float *d_out, uns
     const int g_col = p_cols ? persistent_grid((const void *)ck.p_col, ck.p_threads, ck.p_smem, J.n_col_tiles) : 0;
     ck.init<<<J.n_col_tiles, ck.threads, smem_col, s>>>(d_j, d_l + 1);
     for (int c = 0; c <= J.n_cycles; ++c) {
-        rk.finish<<<J.n_row_tiles, rk.threads, smem_fin, s>>>(d_j, d_l, nullptr);
+        if (int rc = launch_finish(rk, J.n_row_tiles, smem_fin, s, d_j, d_l, nullptr)) return rc;
         k_vblur<<<J.n_vb_tiles, kVbThreads, 0, s>>>(d_j, d_l + 2);
         if (c == J.n_cycles) break;   // final pass: error and stop test only
         for (int i = 0; i < J.n_hio; ++i) {
