@@ -1003,6 +1003,316 @@ __global__ void __launch_bounds__(rcol_threads(N)) k_fft_cols_r(float2 *data, Ff
     }
 }
 
+// ---------------------------------------------------------------- Bluestein, in registers
+// Lengths n with a prime factor > 7 run Bluestein's chirp-z transform on the
+// power-of-two work length M >= 2n - 1 (x_j c_j, c the chirp -- conjugated
+// for inverse transforms -- zero-padded to M; FFT_M; times the kernel
+// spectrum; inverse FFT_M; times c_j).  Here the whole chain stays in
+// registers at the positions j = l + m*M/8 of the register FFT, so a row pass
+// keeps g' in registers from the inverse transform through the HIO update to
+// the forward transform, as for power-of-two lengths.  Positions j >= n carry
+// nothing on output.
+template <int M, int NB, bool COLS, int S>
+__device__ __forceinline__ void reg_bluestein(float2 (&v)[8], float2 *sm, int b, int l, const FftPlanDev &p)
+{
+    constexpr int Q = M / 8;
+    const int n = p.n;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        const int j = l + m * Q;
+        if (j < n) {
+            float2 c = __ldg(p.chirp + j);
+            if (S > 0) c.y = -c.y;
+            v[m] = cmul(v[m], c);
+        } else {
+            v[m] = make_float2(0.f, 0.f);
+        }
+    }
+    reg_fft<M, NB, COLS, -1>(v, sm, b, l, p.tw);
+    const float2 *spec = S < 0 ? p.bspec_f : p.bspec_b;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) v[m] = cmul(v[m], __ldg(spec + l + m * Q));
+    reg_fft<M, NB, COLS, +1>(v, sm, b, l, p.tw);
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        const int j = l + m * Q;
+        if (j < n) {
+            float2 c = __ldg(p.chirp + j);
+            if (S > 0) c.y = -c.y;
+            v[m] = cmul(v[m], c);
+        }
+    }
+}
+
+// row pass (see k_row_hio) on Bluestein row lengths: NB rows of length W per CTA
+template <bool FIRST, int M, bool FIX = false>
+__device__ __forceinline__ void b_row_hio_bs(const JobDev *jobs, const WorkItem wi)
+{
+    extern __shared__ float4 smem4[];
+    float2 *sm = reinterpret_cast<float2 *>(smem4);
+    constexpr int NB = rrow_nb(M), Q = M / 8;
+    const JobDev &J = jobs[wi.job];
+    JobState *st = J.st;
+    if (st->stop) return;
+    const int W = J.W;
+    const int b = threadIdx.x / Q, l = threadIdx.x % Q;
+    const int y = wi.tile * J.rpc + b;
+    const bool ok = b < J.rpc && y < J.H;
+    const size_t base = (size_t)y * W;
+    float2 v[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        const int j = l + m * Q;
+        v[m] = ok && j < W ? J.X[base + j] : make_float2(0.f, 0.f);
+    }
+    reg_bluestein<M, NB, false, +1>(v, sm, b, l, J.prow);
+    const float beta = J.beta;
+    const float thr = st->thr;
+    const int k = FIX ? st->cycle : 0;
+    const bool init_gprev = FIX ? k == 0 : FIRST && st->hio_cycle == 0;
+    const bool fin = FIX && k >= J.n_cycles;
+    const bool track = FIX && (J.target > 0.f || fin);
+    double tot = 0.0, cnt = 0.0;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        const int j = l + m * Q;
+        if (!ok || j >= W) continue;
+        const size_t idx = base + j;
+        const float2 gp1 = v[m];
+        uint8_t msk;
+        if (FIRST) {
+            msk = J.vb[idx] < thr ? 1 : 0;
+            J.mask[idx] = msk;
+        } else {
+            msk = J.mask[idx];
+        }
+        if (FIX && track) hio_track(J.out, idx, gp1, msk, tot, cnt);
+        if (fin) continue;
+        const float2 gp = init_gprev ? gp1 : J.G[idx];
+        float2 g;
+        if ((FIX ? msk == 1 : msk != 0) || gp1.x < 0.f)
+            g = make_float2(__fsub_rn(gp.x, __fmul_rn(beta, gp1.x)), __fsub_rn(gp.y, __fmul_rn(beta, gp1.y)));
+        else
+            g = gp1;
+        J.G[idx] = g;
+        v[m] = g;
+    }
+    if (!fin) {
+        reg_bluestein<M, NB, false, -1>(v, sm, b, l, J.prow);
+        if (ok) {
+#pragma unroll
+            for (int m = 0; m < 8; ++m) {
+                const int j = l + m * Q;
+                if (j < W) J.X[base + j] = v[m];
+            }
+        }
+    }
+    if (FIX) hio_tile_done<rrow_threads(M)>(J, wi.tile, tot, cnt);
+}
+template <bool FIRST, int M, bool FIX = false>
+__global__ void __launch_bounds__(rrow_threads(M)) k_row_hio_bs(const JobDev *jobs, const WorkList *L)
+{
+    IMR_ITEM_LOOP((b_row_hio_bs<FIRST, M, FIX>(jobs, wi)));
+}
+
+// once per cycle (see k_row_finish) on Bluestein row lengths
+template <int M>
+__device__ __forceinline__ void b_row_finish_bs(const JobDev *jobs, const WorkItem wi, float2 *dbg_gprime)
+{
+    extern __shared__ float4 smem4[];
+    float2 *sm = reinterpret_cast<float2 *>(smem4);
+    constexpr int NB = rrow_nb(M), T = rrow_threads(M), Q = M / 8;
+    __shared__ float wsm[kTapStride];
+    __shared__ double red[2 * T / 32 > 2 ? 2 * T / 32 : 2];
+    const JobDev &J = jobs[wi.job];
+    JobState *st = J.st;
+    if (st->stop) return;
+    const int c = st->cycle;
+    if (wi.tile == 0 && threadIdx.x == 0) st->max_bits = 0u;
+    const int W = J.W;
+    const int b = threadIdx.x / Q, l = threadIdx.x % Q;
+    const int y = wi.tile * J.rpc + b;
+    const bool ok = b < J.rpc && y < J.H;
+    const size_t base = (size_t)y * W;
+    const int K = J.ntaps[c];
+    if (threadIdx.x < kTapStride) wsm[threadIdx.x] = J.weights[(size_t)c * kTapStride + threadIdx.x];
+    float2 v[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        const int j = l + m * Q;
+        v[m] = ok && j < W ? J.X[base + j] : make_float2(0.f, 0.f);
+    }
+    reg_bluestein<M, NB, false, +1>(v, sm, b, l, J.prow);   // ends with a barrier: sm is free
+    float *nrow = reinterpret_cast<float *>(sm) + b * M;
+    double tot = 0.0, cnt = 0.0;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        const int j = l + m * Q;
+        if (j >= W) continue;
+        const float nv = cnorm_ref(v[m]);
+        nrow[j] = nv;
+        if (ok) {
+            const size_t idx = base + j;
+            J.out[idx] = v[m].x;
+            if (dbg_gprime) dbg_gprime[idx] = v[m];
+            if (c > 0 && J.mask[idx]) {
+                tot += (double)nv;
+                cnt += 1.0;
+            }
+        }
+    }
+    block_sum2<T>(tot, cnt, red);   // includes barriers: nrow complete after it
+    if (threadIdx.x == 0) {
+        J.err_part[2 * wi.tile] = tot;
+        J.err_part[2 * wi.tile + 1] = cnt;
+    }
+    if (ok) {
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            const int j = l + m * Q;
+            if (j < W) J.hb[base + j] = hblur_at(nrow, W, j, wsm, K);
+        }
+    }
+}
+template <int M>
+__global__ void __launch_bounds__(rrow_threads(M)) k_row_finish_bs(const JobDev *jobs, const WorkList *L,
+                                                                   float2 *dbg_gprime)
+{
+    IMR_ITEM_LOOP((b_row_finish_bs<M>(jobs, wi, dbg_gprime)));
+}
+
+// X := inverse column transform of (M, 0), Bluestein column lengths
+template <int M>
+__device__ __forceinline__ void b_col_init_bs(const JobDev *jobs, const WorkItem wi)
+{
+    extern __shared__ float4 smem4[];
+    float2 *sm = reinterpret_cast<float2 *>(smem4);
+    constexpr int NB = rcol_nb(M), Q = M / 8;
+    const JobDev &J = jobs[wi.job];
+    const int W = J.W, H = J.H;
+    const int b = threadIdx.x % NB, l = threadIdx.x / NB;
+    const int x = wi.tile * J.cpc + b;
+    const bool ok = b < J.cpc && x < W;
+    float2 v[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        const int j = l + m * Q;
+        v[m] = make_float2(ok && j < H ? J.M[(size_t)j * W + x] : 0.f, 0.f);
+    }
+    reg_bluestein<M, NB, true, +1>(v, sm, b, l, J.pcol);
+    if (ok) {
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            const int j = l + m * Q;
+            if (j < H) J.X[(size_t)j * W + x] = v[m];
+        }
+    }
+}
+template <int M>
+__global__ void __launch_bounds__(rcol_threads(M)) k_col_init_bs(const JobDev *jobs, const WorkList *L)
+{
+    IMR_ITEM_LOOP((b_col_init_bs<M>(jobs, wi)));
+}
+
+// column pass (see k_col) on Bluestein column lengths
+template <int M>
+__device__ __forceinline__ void b_col_bs(const JobDev *jobs, const WorkItem wi)
+{
+    extern __shared__ float4 smem4[];
+    float2 *sm = reinterpret_cast<float2 *>(smem4);
+    constexpr int NB = rcol_nb(M), Q = M / 8;
+    const JobDev &J = jobs[wi.job];
+    if (J.st->stop) return;
+    const int W = J.W, H = J.H;
+    const int b = threadIdx.x % NB, l = threadIdx.x / NB;
+    const int x = wi.tile * J.cpc + b;
+    const bool ok = b < J.cpc && x < W;
+    const bool guard = J.mode == kModeShrinkWrap;
+    float2 v[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        const int j = l + m * Q;
+        v[m] = ok && j < H ? J.X[(size_t)j * W + x] : make_float2(0.f, 0.f);
+    }
+    reg_bluestein<M, NB, true, -1>(v, sm, b, l, J.pcol);
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        const int j = l + m * Q;
+        const float mod = ok && j < H ? J.M[(size_t)j * W + x] : 0.f;
+        float nrm = cnorm_ref(v[m]);
+        if (nrm == 0.f && guard) nrm = 1.f;
+        const float f = __fdiv_rn(mod, nrm);
+        v[m] = make_float2(__fmul_rn(v[m].x, f), __fmul_rn(v[m].y, f));
+    }
+    reg_bluestein<M, NB, true, +1>(v, sm, b, l, J.pcol);
+    if (ok) {
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            const int j = l + m * Q;
+            if (j < H) J.X[(size_t)j * W + x] = v[m];
+        }
+    }
+}
+template <int M>
+__global__ void __launch_bounds__(rcol_threads(M)) k_col_bs(const JobDev *jobs, const WorkList *L)
+{
+    IMR_ITEM_LOOP((b_col_bs<M>(jobs, wi)));
+}
+
+// plain 2D transform passes on Bluestein lengths (rows of length p.n)
+template <int S, int M>
+__global__ void __launch_bounds__(rrow_threads(M)) k_fft_rows_bs(float2 *data, FftPlanDev p, int H, int rpc)
+{
+    extern __shared__ float4 smem4[];
+    float2 *sm = reinterpret_cast<float2 *>(smem4);
+    constexpr int Q = M / 8;
+    const int n = p.n;
+    const int b = threadIdx.x / Q, l = threadIdx.x % Q;
+    const int y = blockIdx.x * rpc + b;
+    const bool ok = b < rpc && y < H;
+    const size_t base = (size_t)y * n;
+    float2 v[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        const int j = l + m * Q;
+        v[m] = ok && j < n ? data[base + j] : make_float2(0.f, 0.f);
+    }
+    reg_bluestein<M, rrow_nb(M), false, S>(v, sm, b, l, p);
+    if (ok) {
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            const int j = l + m * Q;
+            if (j < n) data[base + j] = v[m];
+        }
+    }
+}
+
+template <int S, int M>
+__global__ void __launch_bounds__(rcol_threads(M)) k_fft_cols_bs(float2 *data, FftPlanDev p, int W, int cpc)
+{
+    extern __shared__ float4 smem4[];
+    float2 *sm = reinterpret_cast<float2 *>(smem4);
+    constexpr int NB = rcol_nb(M), Q = M / 8;
+    const int n = p.n;
+    const int b = threadIdx.x % NB, l = threadIdx.x / NB;
+    const int x = blockIdx.x * cpc + b;
+    const bool ok = b < cpc && x < W;
+    float2 v[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        const int j = l + m * Q;
+        v[m] = ok && j < n ? data[(size_t)j * W + x] : make_float2(0.f, 0.f);
+    }
+    reg_bluestein<M, NB, true, S>(v, sm, b, l, p);
+    if (ok) {
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            const int j = l + m * Q;
+            if (j < n) data[(size_t)j * W + x] = v[m];
+        }
+    }
+}
+
 }  // namespace imr
 
 // ============================================================================
