@@ -239,6 +239,12 @@ static RowKernels row_set()
         k.p_hio_fix = k_row_hio_p<false, N, true>;
         k.p_finish = k_row_finish_p<N>;
         k.p_smem_fin = pfin_smem<N>();
+    } else if constexpr (N < 0 && -N >= 256) {   // Bluestein lengths, 16 values per thread
+        constexpr int M = -N;
+        k = RowKernels{k_row_hio_bs16<true, M>, k_row_hio_bs16<false, M>, k_row_finish_bs16<M>,
+                       k_fft_rows_bs16<-1, M>, k_fft_rows_bs16<+1, M>, bs16_rows(M), bs16_row_threads(M),
+                       bs16_row_smem(M), nullptr, nullptr, 0, 0, M};
+        k.hio_fix = k_row_hio_bs16<false, M, true>;
     } else if constexpr (N < 0 && -N >= 8) {   // Bluestein lengths: register chirp-z transforms
         constexpr int M = -N;
         k = RowKernels{k_row_hio_bs<true, M>, k_row_hio_bs<false, M>, k_row_finish_bs<M>, k_fft_rows_bs<-1, M>,
@@ -272,6 +278,9 @@ static ColKernels col_set()
         return ColKernels{k_col<N>, k_col_init<N>, k_fft_cols<-1, N>, k_fft_cols<+1, N>, col_nb(N),
                           col_threads(N), 0, k_col_p<N>, pcol_smem<N>(), pcol_box_rows(N),
                           pcol_tma_m(N) ? 1 : 0, pcol_threads(N), 0, rcol_nb(N)};
+    else if constexpr (N < 0 && -N >= 256)   // Bluestein lengths, 16 values per thread
+        return ColKernels{k_col_bs16<-N, 0>, k_col_bs16<-N, 1>, k_fft_cols_bs16<-1, -N>, k_fft_cols_bs16<+1, -N>,
+                          rcol_nb(-N), bs16_col_threads(-N), bs16_col_smem(-N), nullptr, 0, 0, 0, 0, -N, 0};
     else if constexpr (N < 0 && -N >= 8)   // Bluestein lengths: register chirp-z transforms
         return ColKernels{k_col_bs<-N>, k_col_init_bs<-N>, k_fft_cols_bs<-1, -N>, k_fft_cols_bs<+1, -N>,
                           rcol_nb(-N), rcol_threads(-N), rcol_smem(-N), nullptr, 0, 0, 0, 0, -N, 0};

@@ -446,6 +446,13 @@ struct ColSwz16 {
     __device__ __forceinline__ static int at(int b, int e) { return (e ^ ((e >> 4) & (16 / NB - 1))) * NB + b; }
 };
 
+// Row layout of the 16-value exchanges: sequence b at b*N, element e at
+// e ^ ((e >> 4) & 15) (the column-tile swizzle with one column per tile).
+template <int N>
+struct RowSwz16 {
+    __device__ __forceinline__ static int at(int b, int e) { return b * N + (e ^ ((e >> 4) & 15)); }
+};
+
 template <int N, class LAYOUT, int S, int P, int NS>
 __device__ __forceinline__ void reg16_passes(float2 (&v)[16], float2 *buf, int b, int l, const RegTw16<N> &tw)
 {

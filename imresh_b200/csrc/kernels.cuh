@@ -1313,6 +1313,290 @@ __global__ void __launch_bounds__(rcol_threads(M)) k_fft_cols_bs(float2 *data, F
     }
 }
 
+// ---- Bluestein with 16 values per thread (work lengths M >= 256) ------------
+// The same chain as reg_bluestein on the 16-value register FFT: two
+// exchanges per length-M transform up to M = 4096 instead of three, and
+// twiddle powers in registers (loaded once per CTA; every job of a launch has
+// the same work length).  Rows: 4096/M rows per CTA (256 threads); column
+// tiles: rcol_nb(M) columns (512 threads for M >= 512).
+__host__ __device__ constexpr int bs16_rows(int M) { return M >= 4096 ? 1 : 4096 / M; }
+__host__ __device__ constexpr int bs16_row_threads(int M) { return bs16_rows(M) * M / 16; }
+__host__ __device__ constexpr int bs16_row_smem(int M) { return bs16_rows(M) * M * 8; }
+__host__ __device__ constexpr int bs16_col_threads(int M) { return rcol_nb(M) * M / 16; }
+__host__ __device__ constexpr int bs16_col_smem(int M) { return rcol_nb(M) * M * 8; }
+
+template <int M, class LAYOUT, int S>
+__device__ __forceinline__ void reg16_bluestein(float2 (&v)[16], float2 *sm, int b, int l, const RegTw16<M> &tw,
+                                                const FftPlanDev &p)
+{
+    constexpr int Q = M / 16;
+    const int n = p.n;
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+        const int j = l + m * Q;
+        if (j < n) {
+            float2 c = __ldg(p.chirp + j);
+            if (S > 0) c.y = -c.y;
+            v[m] = cmul(v[m], c);
+        } else {
+            v[m] = make_float2(0.f, 0.f);
+        }
+    }
+    reg16_fft<M, LAYOUT, -1>(v, sm, b, l, tw);
+    const float2 *spec = S < 0 ? p.bspec_f : p.bspec_b;
+#pragma unroll
+    for (int m = 0; m < 16; ++m) v[m] = cmul(v[m], __ldg(spec + l + m * Q));
+    reg16_fft<M, LAYOUT, +1>(v, sm, b, l, tw);
+    __syncthreads();   // the last exchange's reads are done before the buffer is written again
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+        const int j = l + m * Q;
+        if (j < n) {
+            float2 c = __ldg(p.chirp + j);
+            if (S > 0) c.y = -c.y;
+            v[m] = cmul(v[m], c);
+        }
+    }
+}
+
+template <bool FIRST, int M, bool FIX = false>
+__global__ void __launch_bounds__(bs16_row_threads(M), 2) k_row_hio_bs16(const JobDev *jobs, const WorkList *L)
+{
+    extern __shared__ float4 smem4[];
+    float2 *sm = reinterpret_cast<float2 *>(smem4);
+    constexpr int Q = M / 16, T = bs16_row_threads(M);
+    const int b = threadIdx.x / Q, l = threadIdx.x % Q;
+    const int n_items = L->n;
+    if ((int)blockIdx.x >= n_items) return;
+    RegTw16<M> rtw;
+    rtw.load(jobs[item_at(L, blockIdx.x).job].prow.tw, l);
+    for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+        const WorkItem wi = item_at(L, it);
+        const JobDev &J = jobs[wi.job];
+        JobState *st = J.st;
+        if (st->stop) continue;
+        const int W = J.W;
+        const int y = wi.tile * J.rpc + b;
+        const bool ok = b < J.rpc && y < J.H;
+        const size_t base = (size_t)y * W;
+        float2 v[16];
+#pragma unroll
+        for (int m = 0; m < 16; ++m) {
+            const int j = l + m * Q;
+            v[m] = ok && j < W ? J.X[base + j] : make_float2(0.f, 0.f);
+        }
+        reg16_bluestein<M, RowSwz16<M>, +1>(v, sm, b, l, rtw, J.prow);
+        const float beta = J.beta;
+        const float thr = st->thr;
+        const int k = FIX ? st->cycle : 0;
+        const bool init_gprev = FIX ? k == 0 : FIRST && st->hio_cycle == 0;
+        const bool fin = FIX && k >= J.n_cycles;
+        const bool track = FIX && (J.target > 0.f || fin);
+        double tot = 0.0, cnt = 0.0;
+#pragma unroll
+        for (int m = 0; m < 16; ++m) {
+            const int j = l + m * Q;
+            if (!ok || j >= W) continue;
+            const size_t idx = base + j;
+            const float2 gp1 = v[m];
+            uint8_t msk;
+            if (FIRST) {
+                msk = J.vb[idx] < thr ? 1 : 0;
+                J.mask[idx] = msk;
+            } else {
+                msk = J.mask[idx];
+            }
+            if (FIX && track) hio_track(J.out, idx, gp1, msk, tot, cnt);
+            if (fin) continue;
+            const float2 gp = init_gprev ? gp1 : J.G[idx];
+            float2 g;
+            if ((FIX ? msk == 1 : msk != 0) || gp1.x < 0.f)
+                g = make_float2(__fsub_rn(gp.x, __fmul_rn(beta, gp1.x)), __fsub_rn(gp.y, __fmul_rn(beta, gp1.y)));
+            else
+                g = gp1;
+            J.G[idx] = g;
+            v[m] = g;
+        }
+        if (!fin) {
+            reg16_bluestein<M, RowSwz16<M>, -1>(v, sm, b, l, rtw, J.prow);
+            if (ok) {
+#pragma unroll
+                for (int m = 0; m < 16; ++m) {
+                    const int j = l + m * Q;
+                    if (j < W) J.X[base + j] = v[m];
+                }
+            }
+        }
+        if (FIX) hio_tile_done<T>(J, wi.tile, tot, cnt);
+        __syncthreads();
+    }
+}
+
+template <int M>
+__global__ void __launch_bounds__(bs16_row_threads(M), 2) k_row_finish_bs16(const JobDev *jobs, const WorkList *L,
+                                                                         float2 *dbg_gprime)
+{
+    extern __shared__ float4 smem4[];
+    float2 *sm = reinterpret_cast<float2 *>(smem4);
+    constexpr int Q = M / 16, T = bs16_row_threads(M);
+    __shared__ float wsm[kTapStride];
+    __shared__ double red[2 * T / 32 > 2 ? 2 * T / 32 : 2];
+    const int b = threadIdx.x / Q, l = threadIdx.x % Q;
+    const int n_items = L->n;
+    if ((int)blockIdx.x >= n_items) return;
+    RegTw16<M> rtw;
+    rtw.load(jobs[item_at(L, blockIdx.x).job].prow.tw, l);
+    for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+        const WorkItem wi = item_at(L, it);
+        const JobDev &J = jobs[wi.job];
+        JobState *st = J.st;
+        if (st->stop) continue;
+        const int c = st->cycle;
+        if (wi.tile == 0 && threadIdx.x == 0) st->max_bits = 0u;
+        const int W = J.W;
+        const int y = wi.tile * J.rpc + b;
+        const bool ok = b < J.rpc && y < J.H;
+        const size_t base = (size_t)y * W;
+        const int K = J.ntaps[c];
+        if (threadIdx.x < kTapStride) wsm[threadIdx.x] = J.weights[(size_t)c * kTapStride + threadIdx.x];
+        float2 v[16];
+#pragma unroll
+        for (int m = 0; m < 16; ++m) {
+            const int j = l + m * Q;
+            v[m] = ok && j < W ? J.X[base + j] : make_float2(0.f, 0.f);
+        }
+        reg16_bluestein<M, RowSwz16<M>, +1>(v, sm, b, l, rtw, J.prow);   // ends with a barrier: sm is free
+        float *nrow = reinterpret_cast<float *>(sm) + b * M;
+        double tot = 0.0, cnt = 0.0;
+#pragma unroll
+        for (int m = 0; m < 16; ++m) {
+            const int j = l + m * Q;
+            if (j >= W) continue;
+            const float nv = cnorm_ref(v[m]);
+            nrow[j] = nv;
+            if (ok) {
+                const size_t idx = base + j;
+                J.out[idx] = v[m].x;
+                if (dbg_gprime) dbg_gprime[idx] = v[m];
+                if (c > 0 && J.mask[idx]) {
+                    tot += (double)nv;
+                    cnt += 1.0;
+                }
+            }
+        }
+        block_sum2<T>(tot, cnt, red);   // includes barriers: nrow complete after it
+        if (threadIdx.x == 0) {
+            J.err_part[2 * wi.tile] = tot;
+            J.err_part[2 * wi.tile + 1] = cnt;
+        }
+        if (ok) {
+#pragma unroll
+            for (int m = 0; m < 16; ++m) {
+                const int j = l + m * Q;
+                if (j < W) J.hb[base + j] = hblur_at(nrow, W, j, wsm, K);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// column kernels: mode 0 column pass (fwd, modulus, inv), 1 column init
+// (inverse of (M, 0)), 2 plain forward, 3 plain inverse
+template <int M, int MODE>
+__device__ __forceinline__ void col_bs16_tile(float2 *X, const float *Mod, int W, int H, int x0, int cpc,
+                                              const FftPlanDev &p, const RegTw16<M> &rtw, bool guard)
+{
+    extern __shared__ float4 smem4[];
+    float2 *sm = reinterpret_cast<float2 *>(smem4);
+    constexpr int NB = rcol_nb(M), Q = M / 16;
+    const int b = threadIdx.x % NB, l = threadIdx.x / NB;
+    const int x = x0 + b;
+    const bool ok = b < cpc && x < W;
+    float2 v[16];
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+        const int j = l + m * Q;
+        if (MODE == 1) v[m] = make_float2(ok && j < H ? Mod[(size_t)j * W + x] : 0.f, 0.f);
+        else v[m] = ok && j < H ? X[(size_t)j * W + x] : make_float2(0.f, 0.f);
+    }
+    if (MODE == 0) {
+        reg16_bluestein<M, ColSwz16<M, NB>, -1>(v, sm, b, l, rtw, p);
+#pragma unroll
+        for (int m = 0; m < 16; ++m) {
+            const int j = l + m * Q;
+            const float mod = ok && j < H ? Mod[(size_t)j * W + x] : 0.f;
+            float nrm = cnorm_ref(v[m]);
+            if (nrm == 0.f && guard) nrm = 1.f;
+            const float f = __fdiv_rn(mod, nrm);
+            v[m] = make_float2(__fmul_rn(v[m].x, f), __fmul_rn(v[m].y, f));
+        }
+    }
+    reg16_bluestein<M, ColSwz16<M, NB>, MODE == 2 ? -1 : +1>(v, sm, b, l, rtw, p);
+    if (ok) {
+#pragma unroll
+        for (int m = 0; m < 16; ++m) {
+            const int j = l + m * Q;
+            if (j < H) X[(size_t)j * W + x] = v[m];
+        }
+    }
+}
+
+template <int M, int MODE>
+__global__ void __launch_bounds__(bs16_col_threads(M)) k_col_bs16(const JobDev *jobs, const WorkList *L)
+{
+    constexpr int NB = rcol_nb(M);
+    const int n_items = L->n;
+    if ((int)blockIdx.x >= n_items) return;
+    RegTw16<M> rtw;
+    rtw.load(jobs[item_at(L, blockIdx.x).job].pcol.tw, threadIdx.x / NB);
+    for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+        const WorkItem wi = item_at(L, it);
+        const JobDev &J = jobs[wi.job];
+        if (MODE == 0 && J.st->stop) continue;
+        col_bs16_tile<M, MODE>(J.X, J.M, J.W, J.H, wi.tile * J.cpc, J.cpc, J.pcol, rtw,
+                               J.mode == kModeShrinkWrap);
+        __syncthreads();
+    }
+}
+
+template <int S, int M>
+__global__ void __launch_bounds__(bs16_row_threads(M), 2) k_fft_rows_bs16(float2 *data, FftPlanDev p, int H, int rpc)
+{
+    extern __shared__ float4 smem4[];
+    float2 *sm = reinterpret_cast<float2 *>(smem4);
+    constexpr int Q = M / 16;
+    const int n = p.n;
+    const int b = threadIdx.x / Q, l = threadIdx.x % Q;
+    const int y = blockIdx.x * rpc + b;
+    const bool ok = b < rpc && y < H;
+    const size_t base = (size_t)y * n;
+    RegTw16<M> rtw;
+    rtw.load(p.tw, l);
+    float2 v[16];
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+        const int j = l + m * Q;
+        v[m] = ok && j < n ? data[base + j] : make_float2(0.f, 0.f);
+    }
+    reg16_bluestein<M, RowSwz16<M>, S>(v, sm, b, l, rtw, p);
+    if (ok) {
+#pragma unroll
+        for (int m = 0; m < 16; ++m) {
+            const int j = l + m * Q;
+            if (j < n) data[base + j] = v[m];
+        }
+    }
+}
+
+template <int S, int M>
+__global__ void __launch_bounds__(bs16_col_threads(M)) k_fft_cols_bs16(float2 *data, FftPlanDev p, int W, int cpc)
+{
+    constexpr int NB = rcol_nb(M);
+    RegTw16<M> rtw;
+    rtw.load(p.tw, threadIdx.x / NB);
+    col_bs16_tile<M, S < 0 ? 2 : 3>(data, nullptr, W, p.n, blockIdx.x * cpc, cpc, p, rtw, true);
+}
+
 }  // namespace imr
 
 // ============================================================================
