@@ -541,6 +541,8 @@ int fft_passes(float2 *d, int W, int H, int sign, int axes, const FftPlanDev &pr
 using namespace imr;
 
 // ==================================================================== plans
+constexpr int kPlanGraphCycles = 64;   // shrink-wrap cycles per captured graph
+
 struct imr_plan {
     int dev = 0;
     int W = 0, H = 0;
@@ -550,8 +552,11 @@ struct imr_plan {
     JobState *st = nullptr;
     void *arena = nullptr;
     size_t smem_row = 0, smem_fin = 0, smem_col = 0;
-    cudaGraphExec_t gexec = nullptr;
-    cudaGraph_t graph = nullptr;
+    // the cycles of one execution as at most two captured graphs: `chunk`
+    // cycles replayed n_chunks times, then the remaining cycles
+    cudaGraphExec_t gexec = nullptr, gexec_rem = nullptr;
+    cudaGraph_t graph = nullptr, graph_rem = nullptr;
+    int chunk = 0, n_chunks = 0;
     float2 *dbg_gprime = nullptr;
     RowKernels rk{};
     ColKernels ck{};
@@ -738,6 +743,8 @@ int imr_plan_destroy(imr_plan *P)
     if (!P) return IMR_SUCCESS;
     if (P->gexec) cudaGraphExecDestroy(P->gexec);
     if (P->graph) cudaGraphDestroy(P->graph);
+    if (P->gexec_rem) cudaGraphExecDestroy(P->gexec_rem);
+    if (P->graph_rem) cudaGraphDestroy(P->graph_rem);
     if (P->arena) cudaFree(P->arena);
     if (P->dbg_gprime) cudaFree(P->dbg_gprime);
     delete P;
@@ -801,15 +808,25 @@ int imr_plan_create(imr_plan **out, unsigned W, unsigned H, const imr_params *pa
         imr_plan_destroy(P);
         return IMR_ERR_CUDA;
     }
-    // capture one shrink-wrap cycle as a graph
+    // capture the cycles as graphs: up to kPlanGraphCycles cycles per graph, so a
+    // reconstruction is one or a few graph launches (no host work between
+    // cycles), plus one graph for the remainder
+    P->chunk = J.n_cycles < kPlanGraphCycles ? J.n_cycles : kPlanGraphCycles;
+    P->n_chunks = P->chunk ? J.n_cycles / P->chunk : 0;
+    const int rem = P->chunk ? J.n_cycles % P->chunk : 0;
     cudaStream_t cs;
     e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
-    if (e == cudaSuccess) {
-        rc = plan_launch_cycle(P, cs);
-        cudaError_t e2 = cudaStreamEndCapture(cs, &P->graph);
+    for (int g = 0; g < 2 && e == cudaSuccess && rc == IMR_SUCCESS; ++g) {
+        const int cycles = g == 0 ? P->chunk : rem;
+        if (cycles == 0) continue;
+        cudaGraph_t &gr = g == 0 ? P->graph : P->graph_rem;
+        cudaGraphExec_t &gx = g == 0 ? P->gexec : P->gexec_rem;
+        e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) break;
+        for (int c = 0; c < cycles && rc == IMR_SUCCESS; ++c) rc = plan_launch_cycle(P, cs);
+        cudaError_t e2 = cudaStreamEndCapture(cs, &gr);
         if (rc == IMR_SUCCESS && e2 == cudaSuccess)
-            e = cudaGraphInstantiate(&P->gexec, P->graph, 0);
+            e = cudaGraphInstantiate(&gx, gr, 0);
         else if (e2 != cudaSuccess)
             e = e2;
     }
@@ -840,7 +857,8 @@ int imr_plan_execute(imr_plan *P, const float *d_modulus, float *d_out, void *st
     CK(cudaMemsetAsync(P->st, 0, sizeof(JobState), s));
     P->ck.init<<<J.n_col_tiles, P->ck.threads, P->smem_col, s>>>(P->dj, P->Lcol);
     CK(cudaGetLastError());
-    for (int c = 0; c < J.n_cycles; ++c) CK(cudaGraphLaunch(P->gexec, s));
+    for (int c = 0; c < P->n_chunks; ++c) CK(cudaGraphLaunch(P->gexec, s));
+    if (P->gexec_rem) CK(cudaGraphLaunch(P->gexec_rem, s));
     if (int rc = launch_finish(P->rk, J.n_row_tiles, P->smem_fin, s, P->dj, P->Lrow, P->dbg_gprime)) return rc;
     k_vblur<<<J.n_vb_tiles, kVbThreads, 0, s>>>(P->dj, P->Lvb);
     CK(cudaGetLastError());
@@ -858,7 +876,8 @@ int imr_plan_execute_host(imr_plan *P, const float *h_modulus, float *h_out, voi
     CK(cudaMemsetAsync(P->st, 0, sizeof(JobState), s));
     P->ck.init<<<J.n_col_tiles, P->ck.threads, P->smem_col, s>>>(P->dj, P->Lcol);
     CK(cudaGetLastError());
-    for (int c = 0; c < J.n_cycles; ++c) CK(cudaGraphLaunch(P->gexec, s));
+    for (int c = 0; c < P->n_chunks; ++c) CK(cudaGraphLaunch(P->gexec, s));
+    if (P->gexec_rem) CK(cudaGraphLaunch(P->gexec_rem, s));
     if (int rc = launch_finish(P->rk, J.n_row_tiles, P->smem_fin, s, P->dj, P->Lrow, P->dbg_gprime)) return rc;
     k_vblur<<<J.n_vb_tiles, kVbThreads, 0, s>>>(P->dj, P->Lvb);
     CK(cudaGetLastError());
