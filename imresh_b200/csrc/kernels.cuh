@@ -1630,6 +1630,32 @@ __device__ __forceinline__ bool job_live(const JobDev *jobs, const WorkList *L, 
     return jobs[wi.job].st->stop == 0;
 }
 
+// A persistent CTA's walk over its work items (stride gridDim.x), skipping
+// items of stopped jobs.  A job's stop flag does not change during a launch
+// (only the once-per-cycle kernels write it), so the liveness of the last job
+// looked at is kept: a CTA whose consecutive items belong to one job (always,
+// for a one-job list) pays no dependent global loads per item.
+struct LiveWalker {
+    const JobDev *jobs;
+    const WorkItem *items;
+    int n, job = -1;
+    bool live = false;
+    __device__ LiveWalker(const JobDev *j, const WorkList *L) : jobs(j), items(L->items), n(L->n) {}
+    __device__ __forceinline__ int next(int it)
+    {
+        for (; it < n; it += gridDim.x) {
+            const int jb = items ? items[it].job : 0;
+            if (jb != job) {
+                job = jb;
+                live = jobs[jb].st->stop == 0;
+            }
+            if (live) break;
+        }
+        return it;
+    }
+    __device__ __forceinline__ WorkItem at(int it) const { return items ? items[it] : WorkItem{0, it}; }
+};
+
 // FIX: fixed-support HIO iteration (see b_row_hio)
 template <bool FIRST, int N, bool FIX = false>
 __global__ void __launch_bounds__(rrow_threads(N)) k_row_hio_p(const JobDev *jobs, const WorkList *L)
@@ -1643,12 +1669,10 @@ __global__ void __launch_bounds__(rrow_threads(N)) k_row_hio_p(const JobDev *job
     const int b = threadIdx.x / Q, l = threadIdx.x % Q;
     const int n_items = L->n;
 
-    auto next_live = [&](int it) {
-        while (it < n_items && !job_live(jobs, L, it)) it += gridDim.x;
-        return it;
-    };
+    LiveWalker walk(jobs, L);
+    auto next_live = [&](int it) { return walk.next(it); };
     auto issue = [&](int item, int s) {   // one thread
-        const WorkItem wi = item_at(L, item);
+        const WorkItem wi = walk.at(item);
         const JobDev &J = jobs[wi.job];
         const int y0 = wi.tile * J.rpc;
         const int nr = min(J.rpc, J.H - y0);
@@ -1673,7 +1697,7 @@ __global__ void __launch_bounds__(rrow_threads(N)) k_row_hio_p(const JobDev *job
     if (threadIdx.x == 0 && item < n_items) issue(item, 0);
     // every job of this launch has row length N: one twiddle set for all items
     RegTw<N> rtw;
-    if (item < n_items) rtw.load(jobs[item_at(L, item).job].prow.tw, l);
+    if (item < n_items) rtw.load(jobs[walk.at(item).job].prow.tw, l);
     for (int k = 0; item < n_items; ++k) {
         const int s = k & 1;
         int nxt = n_items;
@@ -1686,7 +1710,7 @@ __global__ void __launch_bounds__(rrow_threads(N)) k_row_hio_p(const JobDev *job
             }
         }
         // this item's job fields, loaded before the wait so that their latency overlaps it
-        const WorkItem wi = item_at(L, item);
+        const WorkItem wi = walk.at(item);
         const JobDev &J = jobs[wi.job];
         JobState *const st = J.st;
         float2 *const Xg = J.X;
@@ -1784,12 +1808,10 @@ __global__ void __launch_bounds__(rrow_threads(N)) k_row_finish_p(const JobDev *
     const int b = threadIdx.x / Q, l = threadIdx.x % Q;
     const int n_items = L->n;
 
-    auto next_live = [&](int it) {
-        while (it < n_items && !job_live(jobs, L, it)) it += gridDim.x;
-        return it;
-    };
+    LiveWalker walk(jobs, L);
+    auto next_live = [&](int it) { return walk.next(it); };
     auto issue = [&](int item, int s) {   // one thread
-        const WorkItem wi = item_at(L, item);
+        const WorkItem wi = walk.at(item);
         const JobDev &J = jobs[wi.job];
         const int y0 = wi.tile * J.rpc;
         const int nr = min(J.rpc, J.H - y0);
@@ -1809,7 +1831,7 @@ __global__ void __launch_bounds__(rrow_threads(N)) k_row_finish_p(const JobDev *
     int item = next_live(blockIdx.x);
     if (threadIdx.x == 0 && item < n_items) issue(item, 0);
     RegTw<N> rtw;
-    if (item < n_items) rtw.load(jobs[item_at(L, item).job].prow.tw, l);
+    if (item < n_items) rtw.load(jobs[walk.at(item).job].prow.tw, l);
     for (int k = 0; item < n_items; ++k) {
         const int s = k & 1;
         int nxt = n_items;
@@ -1821,7 +1843,7 @@ __global__ void __launch_bounds__(rrow_threads(N)) k_row_finish_p(const JobDev *
                 issue(nxt, s ^ 1);
             }
         }
-        const WorkItem wi = item_at(L, item);
+        const WorkItem wi = walk.at(item);
         const JobDev &J = jobs[wi.job];
         JobState *const st = J.st;
         float *const outp = J.out;
@@ -1913,12 +1935,10 @@ __global__ void __launch_bounds__(rcol_threads(N)) k_col_p(const JobDev *jobs, c
     const int b = threadIdx.x % NB, l = threadIdx.x / NB;
     const int n_items = L->n;
 
-    auto next_live = [&](int it) {
-        while (it < n_items && !job_live(jobs, L, it)) it += gridDim.x;
-        return it;
-    };
+    LiveWalker walk(jobs, L);
+    auto next_live = [&](int it) { return walk.next(it); };
     auto issue = [&](int item, int s) {
-        const WorkItem wi = item_at(L, item);
+        const WorkItem wi = walk.at(item);
         const JobDev &J = jobs[wi.job];
         unsigned char *st = stages + s * STAGE;
         const int x0 = wi.tile * NB;
@@ -1939,7 +1959,7 @@ __global__ void __launch_bounds__(rcol_threads(N)) k_col_p(const JobDev *jobs, c
     }
     int item = next_live(blockIdx.x);
     if (item < n_items) {
-        const float2 *gtw = jobs[item_at(L, item).job].pcol.tw;
+        const float2 *gtw = jobs[walk.at(item).job].pcol.tw;
         for (int i = threadIdx.x; i < N; i += rcol_threads(N)) stw[i] = gtw[i];
     }
     __syncthreads();
@@ -1952,7 +1972,7 @@ __global__ void __launch_bounds__(rcol_threads(N)) k_col_p(const JobDev *jobs, c
             fence_proxy_async_smem();
             issue(nxt, s ^ 1);
         }
-        const WorkItem wi = item_at(L, item);
+        const WorkItem wi = walk.at(item);
         const JobDev &J = jobs[wi.job];
         const bool landed = mbar_wait(&bars[s], (uint32_t)((k >> 1) & 1));
         if (__syncthreads_or(!landed)) {
@@ -2035,12 +2055,10 @@ k_col_p16(const JobDev *jobs, const WorkList *L)
     const int b = threadIdx.x % NB, l = threadIdx.x / NB;
     const int n_items = L->n;
 
-    auto next_live = [&](int it) {
-        while (it < n_items && !job_live(jobs, L, it)) it += gridDim.x;
-        return it;
-    };
+    LiveWalker walk(jobs, L);
+    auto next_live = [&](int it) { return walk.next(it); };
     auto issue = [&](int item, int s) {   // one thread
-        const WorkItem wi = item_at(L, item);
+        const WorkItem wi = walk.at(item);
         const JobDev &J = jobs[wi.job];
         unsigned char *st = stages + s * STAGE;
         const int x0 = wi.tile * NB;
@@ -2059,7 +2077,7 @@ k_col_p16(const JobDev *jobs, const WorkList *L)
     int item = next_live(blockIdx.x);
     // the column length is N for every job of this launch: one set of twiddles
     RegTw16<N> rtw;
-    if (item < n_items) rtw.load(jobs[item_at(L, item).job].pcol.tw, l);
+    if (item < n_items) rtw.load(jobs[walk.at(item).job].pcol.tw, l);
     __syncthreads();
     if (threadIdx.x == 0 && item < n_items) issue(item, 0);
     __shared__ int s_next[2];   // next item, found by thread 0 (double-buffered by iteration parity)
@@ -2070,7 +2088,7 @@ k_col_p16(const JobDev *jobs, const WorkList *L)
             nxt = next_live(item + gridDim.x);
             s_next[s] = nxt;
         }
-        const WorkItem wi = item_at(L, item);
+        const WorkItem wi = walk.at(item);
         const JobDev &J = jobs[wi.job];
         const int W = J.W;
         const int x = wi.tile * NB + b;
