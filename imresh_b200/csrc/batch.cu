@@ -171,6 +171,8 @@ static int admit(imr_engine *E, std::vector<EJob *> &fresh)
         if (j->resume.empty()) {
             CKE(cudaMemsetAsync(E->dst + j->slot, 0, sizeof(JobState), E->s));
             CKE(cudaMemcpyAsync((void *)j->J.M, j->h_in, (size_t)j->W * j->H * 4, cudaMemcpyHostToDevice, E->s));
+            if ((rc = job_modulus_tiles(j->J, E->s))) return rc;
+            if (j->J.Mt) ++E->launches;
             fresh.push_back(j);
         } else {   // continue a suspended reconstruction where it stopped
             const SnapHeader *h = (const SnapHeader *)j->resume.data();
@@ -182,6 +184,8 @@ static int admit(imr_engine *E, std::vector<EJob *> &fresh)
             CKE(cudaMemcpyAsync(j->J.X, d, N * 8, cudaMemcpyHostToDevice, E->s));
             CKE(cudaMemcpyAsync(j->J.G, d + N * 8, N * 8, cudaMemcpyHostToDevice, E->s));
             CKE(cudaMemcpyAsync((void *)j->J.M, d + N * 16, N * 4, cudaMemcpyHostToDevice, E->s));
+            if ((rc = job_modulus_tiles(j->J, E->s))) return rc;
+            if (j->J.Mt) ++E->launches;
             CKE(cudaMemcpyAsync(j->J.mask, d + N * 20, N, cudaMemcpyHostToDevice, E->s));
             CKE(cudaMemcpyAsync(j->J.errors, d + N * 21, (size_t)h->n_err * 4, cudaMemcpyHostToDevice, E->s));
             CKE(cudaStreamSynchronize(E->s));

@@ -266,7 +266,7 @@ static ColKernels col_set()
         constexpr int T = pcol16_nbt(N);
         return ColKernels{k_col_r<N>, k_col_init_r<N>, k_fft_cols_r<-1, N>, k_fft_cols_r<+1, N>,
                           rcol_nb(N), rcol_threads(N), rcol_smem(N), k_col_p16<N, T>, pcol16_smem<N, T>(),
-                          pcol_box_rows(N), T * 4 >= 16 ? 1 : 0, pcol16_threads(N, T), 0, T};
+                          pcol_box_rows(N), 0, pcol16_threads(N, T), 0, T, 1};
     } else if constexpr (N >= 16 && is_pow2(N))
         return ColKernels{k_col_r<N>, k_col_init_r<N>, k_fft_cols_r<-1, N>, k_fft_cols_r<+1, N>,
                           rcol_nb(N), rcol_threads(N), rcol_smem(N), k_col_p<N>, pcol_smem<N>(),
@@ -656,6 +656,10 @@ int job_prepare(unsigned W, unsigned H, const imr_params &p, JobDev &J, JobShape
     S.oX = off; off += al(N * 8);
     S.oG = off; off += al(N * 8);
     S.oM = off; off += al(N * 4);
+    if (S.p_cols && S.ck.p_mt) {
+        S.oMt = off;
+        off += al((size_t)((W + S.ck.p_nb - 1) / S.ck.p_nb) * S.ck.p_nb * H * 4);
+    }
     S.oHB = off; off += al(N * 4);
     S.oVB = off; off += al(N * 4);
     S.oOut = off; off += al(N * 4);
@@ -673,6 +677,7 @@ void job_bind(JobDev &J, JobShape &S, char *a, JobState *st)
     J.X = (float2 *)(a + S.oX);
     J.G = (float2 *)(a + S.oG);
     J.M = (const float *)(a + S.oM);
+    J.Mt = nullptr;
     J.hb = (float *)(a + S.oHB);
     J.vb = (float *)(a + S.oVB);
     J.out = (float *)(a + S.oOut);
@@ -693,7 +698,21 @@ void job_bind(JobDev &J, JobShape &S, char *a, JobState *st)
             J.n_col_tiles = (J.W + J.cpc - 1) / J.cpc;
         }
         J.use_tma_cols = S.p_cols ? 1 : 0;
+        if (S.p_cols && S.ck.p_mt) J.Mt = (const float *)(a + S.oMt);
     }
+}
+
+int job_modulus_tiles(const JobDev &J, cudaStream_t s)
+{
+    if (!J.Mt) return IMR_SUCCESS;
+    const size_t n = (size_t)J.n_col_tiles * J.cpc * J.H;
+    k_modulus_tiles<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(J.M, const_cast<float *>(J.Mt), J.W, J.H, J.cpc, n);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error("modulus tiles", e);
+        return IMR_ERR_CUDA;
+    }
+    return IMR_SUCCESS;
 }
 
 int job_upload(const JobDev &J, const JobShape &S, char *a, JobDev *dj, cudaStream_t s)
@@ -843,7 +862,7 @@ int imr_plan_create(imr_plan **out, unsigned W, unsigned H, const imr_params *pa
 int imr_plan_launches(imr_plan *P, long *launches)
 {
     if (!P || !launches) return IMR_ERR_INVALID_VALUE;
-    *launches = 1 + (long)P->hj.n_cycles * (2 + 2L * P->hj.n_hio) + 2;
+    *launches = (P->hj.Mt ? 2 : 1) + (long)P->hj.n_cycles * (2 + 2L * P->hj.n_hio) + 2;
     return IMR_SUCCESS;
 }
 
@@ -854,6 +873,7 @@ int imr_plan_execute(imr_plan *P, const float *d_modulus, float *d_out, void *st
     const JobDev &J = P->hj;
     const size_t N = (size_t)P->W * P->H;
     CK(cudaMemcpyAsync((void *)J.M, d_modulus, N * 4, cudaMemcpyDeviceToDevice, s));
+    if (int rc = job_modulus_tiles(J, s)) return rc;
     CK(cudaMemsetAsync(P->st, 0, sizeof(JobState), s));
     P->ck.init<<<J.n_col_tiles, P->ck.threads, P->smem_col, s>>>(P->dj, P->Lcol);
     CK(cudaGetLastError());
@@ -873,6 +893,7 @@ int imr_plan_execute_host(imr_plan *P, const float *h_modulus, float *h_out, voi
     const JobDev &J = P->hj;
     const size_t N = (size_t)P->W * P->H;
     CK(cudaMemcpyAsync((void *)J.M, h_modulus, N * 4, cudaMemcpyHostToDevice, s));
+    if (int rc = job_modulus_tiles(J, s)) return rc;
     CK(cudaMemsetAsync(P->st, 0, sizeof(JobState), s));
     P->ck.init<<<J.n_col_tiles, P->ck.threads, P->smem_col, s>>>(P->dj, P->Lcol);
     CK(cudaGetLastError());

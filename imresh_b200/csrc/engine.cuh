@@ -62,6 +62,10 @@ struct alignas(64) JobDev {
     float2 *X;
     float2 *G;
     const float *M;
+    // The modulus in column tiles for the pipelined 16-value column pass, or
+    // null: tile t (columns t*cpc .. t*cpc + cpc - 1) is a contiguous [H][cpc]
+    // block, zero past column W, so a tile arrives by one bulk copy.
+    const float *Mt;
     uint8_t *mask;
     float *hb;
     float *vb;

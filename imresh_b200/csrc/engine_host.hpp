@@ -60,6 +60,7 @@ struct ColKernels {
     int p_threads;   // threads of the pipelined column pass
     int bs_m;        // Bluestein work length (0: direct transform)
     int p_nb;        // columns per tile of the pipelined pass (its TMA box width)
+    int p_mt;        // 1: the pipelined pass reads the modulus from JobDev::Mt when set
 };
 RowKernels row_kernels(int N);
 ColKernels col_kernels(int N);
@@ -83,13 +84,16 @@ struct JobShape {
     bool p_rows = false, p_cols = false;
     size_t smem_row = 0, smem_fin = 0, smem_col = 0;
     size_t bytes = 0;   // arena bytes (JobState not included)
-    size_t oX = 0, oG = 0, oM = 0, oHB = 0, oVB = 0, oOut = 0, oMask = 0, oW = 0, oT = 0, oEP = 0, oErr = 0;
+    size_t oX = 0, oG = 0, oM = 0, oMt = 0, oHB = 0, oVB = 0, oOut = 0, oMask = 0, oW = 0, oT = 0, oEP = 0, oErr = 0;
     std::vector<float> wt;
     std::vector<int> taps;
 };
 int job_prepare(unsigned W, unsigned H, const imr_params &p, JobDev &J, JobShape &S);
 void job_bind(JobDev &J, JobShape &S, char *arena, JobState *st);
 int job_upload(const JobDev &J, const JobShape &S, char *arena, JobDev *dj, cudaStream_t s);
+// Fill JobDev::Mt from the modulus (stream-ordered; nothing to do when Mt is
+// null).  Called whenever the modulus has been (re)written.
+int job_modulus_tiles(const JobDev &J, cudaStream_t s);
 int plan_cache_acquire(unsigned W, unsigned H, const imr_params *params, imr_plan **out);
 void plan_cache_release(imr_plan *P);
 

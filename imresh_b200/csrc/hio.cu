@@ -302,8 +302,9 @@ static int hio_run(imr_hio_plan *P, unsigned seed, cudaStream_t s)
     const JobDev &J = P->hj;
     const long N = (long)P->W * P->H;
     HCK(cudaMemsetAsync(P->st, 0, sizeof(JobState), s));
-    int rc = launch_rand_field(J.X, N, seed, s);
+    int rc = job_modulus_tiles(J, s);
     if (rc) return rc;
+    if ((rc = launch_rand_field(J.X, N, seed, s))) return rc;
     if ((rc = fft_passes(J.X, P->W, P->H, -1, 3, J.prow, J.pcol, s))) return rc;
     const int g = (int)std::min<long>((N + 255) / 256, 148L * 16);
     k_random_phase<<<g, 256, 0, s>>>(J.X, J.M, N);

@@ -107,6 +107,21 @@ __device__ __forceinline__ float cnorm_ref(float2 z)
     return sqrtf(__fadd_rn(__fmul_rn(z.x, z.x), __fmul_rn(z.y, z.y)));
 }
 
+// The modulus projection factor mod / |z| with the reference's rounding
+// (cnorm_ref, then an IEEE division), |z| = 0 taken as 1 when `guard` (the
+// shrink-wrap update; fixed-support HIO divides by the zero).  A zero modulus
+// over a finite nonzero norm is its own quotient, so that case skips the
+// square root and the division: most pixels of a measured diffraction pattern
+// are zero counts (80 % of the 2048^2 benchmark pattern).
+__device__ __forceinline__ float modulus_factor(float mod, float2 z, bool guard)
+{
+    const float ss = __fadd_rn(__fmul_rn(z.x, z.x), __fmul_rn(z.y, z.y));
+    if (mod == 0.f && ss > 0.f && ss < __int_as_float(0x7f800000)) return mod;
+    float nrm = sqrtf(ss);
+    if (nrm == 0.f && guard) nrm = 1.f;
+    return __fdiv_rn(mod, nrm);
+}
+
 // Block-wide sum of two doubles, fixed reduction order (deterministic).
 template <int NT>
 __device__ __forceinline__ void block_sum2(double &a, double &b, double *scratch)
@@ -320,9 +335,7 @@ __device__ __forceinline__ void b_col(const JobDev *jobs, const WorkItem wi)
     for (int i = threadIdx.x; i < H * nc; i += T) {
         const int y = i / nc, c = i - y * nc;
         const float2 g = sm[y * es + c];
-        float nrm = cnorm_ref(g);
-        if (nrm == 0.f && J.mode == kModeShrinkWrap) nrm = 1.f;
-        const float f = __fdiv_rn(J.M[(size_t)y * W + x0 + c], nrm);
+        const float f = modulus_factor(J.M[(size_t)y * W + x0 + c], g, J.mode == kModeShrinkWrap);
         sm[y * es + c] = make_float2(__fmul_rn(g.x, f), __fmul_rn(g.y, f));
     }
     __syncthreads();
@@ -821,9 +834,7 @@ __device__ __forceinline__ void b_col_r(const JobDev *jobs, const WorkItem wi)
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
         const float mod = ok ? J.M[(size_t)(l + m * Q) * W + x] : 0.f;
-        float nrm = cnorm_ref(v[m]);
-        if (nrm == 0.f && J.mode == kModeShrinkWrap) nrm = 1.f;
-        const float f = __fdiv_rn(mod, nrm);
+        const float f = modulus_factor(mod, v[m], J.mode == kModeShrinkWrap);
         v[m] = make_float2(__fmul_rn(v[m].x, f), __fmul_rn(v[m].y, f));
     }
     reg_fft<N, NB, true, +1>(v, sm, b, l, J.pcol.tw);
@@ -1239,9 +1250,7 @@ __device__ __forceinline__ void b_col_bs(const JobDev *jobs, const WorkItem wi)
     for (int m = 0; m < 8; ++m) {
         const int j = l + m * Q;
         const float mod = ok && j < H ? J.M[(size_t)j * W + x] : 0.f;
-        float nrm = cnorm_ref(v[m]);
-        if (nrm == 0.f && guard) nrm = 1.f;
-        const float f = __fdiv_rn(mod, nrm);
+        const float f = modulus_factor(mod, v[m], guard);
         v[m] = make_float2(__fmul_rn(v[m].x, f), __fmul_rn(v[m].y, f));
     }
     reg_bluestein<M, NB, true, +1>(v, sm, b, l, J.pcol);
@@ -1525,9 +1534,7 @@ __device__ __forceinline__ void col_bs16_tile(float2 *X, const float *Mod, int W
         for (int m = 0; m < 16; ++m) {
             const int j = l + m * Q;
             const float mod = ok && j < H ? Mod[(size_t)j * W + x] : 0.f;
-            float nrm = cnorm_ref(v[m]);
-            if (nrm == 0.f && guard) nrm = 1.f;
-            const float f = __fdiv_rn(mod, nrm);
+            const float f = modulus_factor(mod, v[m], guard);
             v[m] = make_float2(__fmul_rn(v[m].x, f), __fmul_rn(v[m].y, f));
         }
     }
@@ -1997,9 +2004,7 @@ __global__ void __launch_bounds__(rcol_threads(N)) k_col_p(const JobDev *jobs, c
             float mod;
             if constexpr (TM) mod = reinterpret_cast<const float *>(stg + XB)[(l + m * Q) * NB + b];
             else mod = ok ? J.M[(size_t)(l + m * Q) * W + x] : 0.f;
-            float nrm = cnorm_ref(v[m]);
-            if (nrm == 0.f && J.mode == kModeShrinkWrap) nrm = 1.f;
-            const float f = __fdiv_rn(mod, nrm);
+            const float f = modulus_factor(mod, v[m], J.mode == kModeShrinkWrap);
             v[m] = make_float2(__fmul_rn(v[m].x, f), __fmul_rn(v[m].y, f));
         }
         reg_fft_1buf<N, ColSwz<N, NB>, +1, true>(v, sX, b, l, stw);
@@ -2020,24 +2025,41 @@ __global__ void __launch_bounds__(rcol_threads(N)) k_col_p(const JobDev *jobs, c
 }
 
 // ---- columns, 16 values per thread (powers of two >= 128) ----------------------
-// The tile, stages and TMA traffic of k_col_p; each thread holds 16 values
-// of its column (a length-2048 transform is three passes, two exchanges),
-// and its twiddle powers stay in registers for the whole persistent loop, so
-// no shared-memory twiddle table (whose strided reads were the pass's bank
-// conflicts) remains.  The next tile is requested after the forward FFT of
-// the current one, when the bulk store that last used its stage has long
-// finished reading it, so the issuing thread does not hold its warp back.
+// The X tiles and TMA traffic of k_col_p; each thread holds 16 values of its
+// column (a length-2048 transform is three passes, two exchanges), and its
+// twiddle powers stay in registers for the whole persistent loop, so no
+// shared-memory twiddle table (whose strided reads were the pass's bank
+// conflicts) remains.  The modulus comes from the job's column-tiled copy
+// (JobDev::Mt: one contiguous block per tile) into registers.  Three stages:
+// tile k+2 is requested after the forward FFT of tile k into the stage of
+// tile k-1, whose bulk store has had a whole forward FFT to read it.
 // (Measured at 2048^2 and kept out: 2-column tiles with two CTAs per SM, 15 %
-// slower; three stages with the modulus fetched into registers, 10 % slower.)
+// slower; the modulus by TMA from the row-major array, 4 % slower.)
+// The modulus in column tiles (JobDev::Mt): element i of the tiled array is
+// tile t = i / (H*NB), row r = (i / NB) % H, column t*NB + i % NB (zero past W).
+static __global__ void k_modulus_tiles(const float *__restrict__ M, float *__restrict__ Mt, int W, int H, int NB, size_t n)
+{
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const size_t t = i / ((size_t)H * NB);
+    const int r = (int)((i / NB) % H), x = (int)(t * NB) + (int)(i % NB);
+    Mt[i] = x < W ? M[(size_t)r * W + x] : 0.f;
+}
+
 __host__ __device__ constexpr int pcol16_threads(int N, int NBT) { return NBT * N / 16; }
 __host__ __device__ constexpr int pcol16_nbt(int N) { return rcol_nb(N); }
+// A stage holds one X tile; the modulus goes straight to registers.  Three
+// stages where they fit (all lengths up to 4096: 64 KB tiles), so tile k+2 is
+// requested while tile k is transformed.
 template <int N, int NBT>
-__host__ __device__ constexpr int pcol16_stage_bytes()
+__host__ __device__ constexpr int pcol16_stage_bytes() { return round128(NBT * N * 8); }
+template <int N, int NBT>
+__host__ __device__ constexpr int pcol16_stages()
 {
-    return round128(NBT * N * 8 + (NBT * 4 >= 16 ? NBT * N * 4 : 0));
+    return 128 + 3 * pcol16_stage_bytes<N, NBT>() <= 227 * 1024 ? 3 : 2;
 }
 template <int N, int NBT>
-__host__ __device__ constexpr int pcol16_smem() { return 128 + 2 * pcol16_stage_bytes<N, NBT>(); }
+__host__ __device__ constexpr int pcol16_smem() { return 128 + pcol16_stages<N, NBT>() * pcol16_stage_bytes<N, NBT>(); }
 __host__ __device__ constexpr int pcol16_min_blocks(int N, int NBT) { return NBT * N / 16 <= 256 ? 2 : 1; }
 
 template <int N, int NBT>
@@ -2048,61 +2070,71 @@ k_col_p16(const JobDev *jobs, const WorkList *L)
     constexpr int NB = NBT, V = 16, Q = N / V;
     constexpr int XB = NB * N * 8;
     constexpr int BR = pcol_box_rows(N);
-    constexpr bool TM = NB * 4 >= 16;   // the modulus tile rows are >= 16 bytes: it comes by TMA too
     constexpr int STAGE = pcol16_stage_bytes<N, NBT>();
-    uint64_t *bars = reinterpret_cast<uint64_t *>(sbuf);
+    constexpr int NST = pcol16_stages<N, NBT>();
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sbuf);   // NST barriers in the first 128 bytes
     unsigned char *stages = sbuf + 128;
     const int b = threadIdx.x % NB, l = threadIdx.x / NB;
     const int n_items = L->n;
+    __shared__ int s_item[NST];   // item whose tile each stage receives (n_items: none); thread 0 writes
 
     LiveWalker walk(jobs, L);
-    auto next_live = [&](int it) { return walk.next(it); };
     auto issue = [&](int item, int s) {   // one thread
         const WorkItem wi = walk.at(item);
         const JobDev &J = jobs[wi.job];
         unsigned char *st = stages + s * STAGE;
         const int x0 = wi.tile * NB;
-        mbar_arrive_expect_tx(&bars[s], (uint32_t)(XB + (TM ? NB * N * 4 : 0)));
-        for (int r0 = 0; r0 < N; r0 += BR) {
-            tma_load_2d(st + (size_t)r0 * NB * 8, &J.tmX, x0, r0, &bars[s]);
-            if constexpr (TM) tma_load_2d(st + XB + (size_t)r0 * NB * 4, &J.tmM, x0, r0, &bars[s]);
-        }
+        mbar_arrive_expect_tx(&bars[s], (uint32_t)XB);
+        for (int r0 = 0; r0 < N; r0 += BR) tma_load_2d(st + (size_t)r0 * NB * 8, &J.tmX, x0, r0, &bars[s]);
     };
 
-    if (threadIdx.x == 0) {
-        mbar_init(&bars[0], 1);
-        mbar_init(&bars[1], 1);
-        mbar_fence_init();
-    }
-    int item = next_live(blockIdx.x);
+    int item = walk.next(blockIdx.x);
     // the column length is N for every job of this launch: one set of twiddles
     RegTw16<N> rtw;
     if (item < n_items) rtw.load(jobs[walk.at(item).job].pcol.tw, l);
-    __syncthreads();
-    if (threadIdx.x == 0 && item < n_items) issue(item, 0);
-    __shared__ int s_next[2];   // next item, found by thread 0 (double-buffered by iteration parity)
-    for (int k = 0; item < n_items; ++k) {
-        const int s = k & 1;
-        int nxt = n_items;
-        if (threadIdx.x == 0) {
-            nxt = next_live(item + gridDim.x);
-            s_next[s] = nxt;
+    int it_next = n_items;   // thread 0: the next item to request
+    if (threadIdx.x == 0) {
+        for (int t = 0; t < NST; ++t) mbar_init(&bars[t], 1);
+        mbar_fence_init();
+        int it = item;
+        for (int t = 0; t < NST - 1; ++t) {   // the first NST - 1 tiles
+            s_item[t] = it;
+            if (it < n_items) {
+                issue(it, t);
+                it = walk.next(it + gridDim.x);
+            }
         }
+        it_next = it;
+    }
+    __syncthreads();
+    for (int k = 0; item < n_items; ++k) {
+        const int s = k % NST;
         const WorkItem wi = walk.at(item);
         const JobDev &J = jobs[wi.job];
         const int W = J.W;
         const int x = wi.tile * NB + b;
         const bool ok = x < W;
         const bool guard = J.mode == kModeShrinkWrap;
+        // the modulus goes straight to registers, its latency hidden by the
+        // tile wait and the forward FFT: from the tiled copy (one 128-byte line
+        // per warp and value) when the job has one
         float mod[V];
-        if constexpr (!TM) {
+        if (const float *mt = J.Mt) {
+            mt += (size_t)wi.tile * NB * N + b;
+#pragma unroll
+            for (int m = 0; m < V; ++m) mod[m] = __ldg(mt + (size_t)(l + m * Q) * NB);
+        } else {
 #pragma unroll
             for (int m = 0; m < V; ++m) mod[m] = ok ? __ldg(J.M + (size_t)(l + m * Q) * W + x) : 0.f;
         }
-        const bool landed = mbar_wait(&bars[s], (uint32_t)((k >> 1) & 1));
+        const bool landed = mbar_wait(&bars[s], (uint32_t)((k / NST) & 1));
         if (__syncthreads_or(!landed)) {
             if (threadIdx.x == 0) {
                 atomicExch(&J.st->err, 1);
+                for (int d = 1; d < NST - 1; ++d) {   // tiles already requested beyond this one
+                    const int t = (k + d) % NST;
+                    if (s_item[t] < n_items) mbar_wait(&bars[t], (uint32_t)(((k + d) / NST) & 1));
+                }
                 bulk_wait0();
             }
             return;
@@ -2113,17 +2145,20 @@ k_col_p16(const JobDev *jobs, const WorkList *L)
 #pragma unroll
         for (int m = 0; m < V; ++m) v[m] = sX[(l + m * Q) * NB + b];
         reg16_fft<N, ColSwz16<N, NB>, -1>(v, sX, b, l, rtw);
-        if (threadIdx.x == 0 && nxt < n_items) {
-            bulk_wait_read0();   // the store of the previous item has left stage s^1
-            fence_proxy_async_smem();
-            issue(nxt, s ^ 1);
+        if (threadIdx.x == 0) {
+            // the stage of tile k - 1: free once the store committed after it has read it
+            const int t = (k + NST - 1) % NST;
+            s_item[t] = it_next;
+            if (it_next < n_items) {
+                bulk_wait_read0();
+                fence_proxy_async_smem();
+                issue(it_next, t);
+                it_next = walk.next(it_next + gridDim.x);
+            }
         }
 #pragma unroll
         for (int m = 0; m < V; ++m) {
-            if constexpr (TM) mod[m] = reinterpret_cast<const float *>(stg + XB)[(l + m * Q) * NB + b];
-            float nrm = cnorm_ref(v[m]);
-            if (nrm == 0.f && guard) nrm = 1.f;
-            const float f = __fdiv_rn(mod[m], nrm);
+            const float f = modulus_factor(mod[m], v[m], guard);
             v[m] = make_float2(__fmul_rn(v[m].x, f), __fmul_rn(v[m].y, f));
         }
         reg16_fft<N, ColSwz16<N, NB>, +1>(v, sX, b, l, rtw);
@@ -2138,7 +2173,7 @@ k_col_p16(const JobDev *jobs, const WorkList *L)
             for (int r0 = 0; r0 < N; r0 += BR) tma_store_2d(&J.tmX, x0, r0, sX + (size_t)r0 * NB);
             bulk_commit();
         }
-        item = s_next[s];   // written before the barriers above
+        item = s_item[(k + 1) % NST];   // written before the barriers above
     }
     if (threadIdx.x == 0) bulk_wait0();
 }
