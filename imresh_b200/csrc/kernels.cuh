@@ -1630,6 +1630,13 @@ __host__ __device__ constexpr int prow_stage_bytes()
 }
 template <bool FIRST, int N>
 __host__ __device__ constexpr int prow_smem() { return 128 + 2 * prow_stage_bytes<FIRST, N>(); }
+// Three 8-warp CTAs per SM for the every-iteration shrink-wrap pass at
+// power-of-two lengths (its stages fit three times in shared memory; 80
+// registers per thread, no spills).  Other variants keep their registers.
+__host__ __device__ constexpr int prow_min_blocks(bool FIRST, bool FIX, int N)
+{
+    return !FIRST && !FIX && is_pow2(N) && N <= 2048 ? 3 : 1;
+}
 
 __device__ __forceinline__ bool job_live(const JobDev *jobs, const WorkList *L, int item)
 {
@@ -1665,7 +1672,7 @@ struct LiveWalker {
 
 // FIX: fixed-support HIO iteration (see b_row_hio)
 template <bool FIRST, int N, bool FIX = false>
-__global__ void __launch_bounds__(rrow_threads(N)) k_row_hio_p(const JobDev *jobs, const WorkList *L)
+__global__ void __launch_bounds__(rrow_threads(N), prow_min_blocks(FIRST, FIX, N)) k_row_hio_p(const JobDev *jobs, const WorkList *L)
 {
     extern __shared__ __align__(128) unsigned char sbuf[];
     constexpr int NB = rrow_nb(N), V = reg_v(N), Q = N / V;
