@@ -247,10 +247,21 @@ __device__ __forceinline__ float vblur_tile(const float *src, float *dst, int W,
     const int tx = threadIdx.x & (kVbTileX - 1);
     const int ty = threadIdx.x / kVbTileX;
     const int x = x0 + tx;
-    for (int r = ty; r < rows_in; r += kVbThreads / kVbTileX) {
+    // all of a thread's tile rows are requested before any is stored, so the
+    // loads' latencies overlap (rows_in <= kVbTileY + 62 for K <= 63 taps)
+    constexpr int RS0 = kVbThreads / kVbTileX, NLD = (kVbTileY + 62 + RS0 - 1) / RS0;
+    float ld[NLD];
+#pragma unroll
+    for (int i = 0; i < NLD; ++i) {
+        const int r = ty + i * RS0;
         int ys = y0 - N + r;
         ys = ys < 0 ? 0 : (ys > H - 1 ? H - 1 : ys);
-        tile[r * kVbTileX + tx] = x < W ? src[(size_t)ys * W + x] : 0.f;
+        ld[i] = r < rows_in && x < W ? __ldg(src + (size_t)ys * W + x) : 0.f;
+    }
+#pragma unroll
+    for (int i = 0; i < NLD; ++i) {
+        const int r = ty + i * RS0;
+        if (r < rows_in) tile[r * kVbTileX + tx] = ld[i];
     }
     __syncthreads();
     // RPT outputs per thread, accumulated side by side (independent chains);
@@ -1908,11 +1919,23 @@ __global__ void __launch_bounds__(rrow_threads(N)) k_row_finish_p(const JobDev *
             J.err_part[2 * wi.tile + 1] = cnt;
         }
         if (ok) {
+            // the V outputs' tap sums side by side (independent chains), each
+            // in the tap order of hblur_at
+            const int hw = (K - 1) / 2;
+            float sum[V];
 #pragma unroll
-            for (int m = 0; m < V; ++m) {
-                const int e = l + m * Q;
-                hbp[base + e] = hblur_at(nrow, N, e, wsm, K);
+            for (int m = 0; m < V; ++m) sum[m] = 0.f;
+            for (int k = 0; k < K; ++k) {
+                const float wk = wsm[k];
+#pragma unroll
+                for (int m = 0; m < V; ++m) {
+                    int xs = l + m * Q - hw + k;
+                    xs = xs < 0 ? 0 : (xs > N - 1 ? N - 1 : xs);
+                    sum[m] = __fadd_rn(sum[m], __fmul_rn(nrow[xs], wk));
+                }
             }
+#pragma unroll
+            for (int m = 0; m < V; ++m) hbp[base + l + m * Q] = sum[m];
         }
         fence_proxy_async_smem();
         __syncthreads();   // stage s is free for the copy issued next iteration; s_next[s] is visible
