@@ -426,6 +426,10 @@ def run_ours(args, rank, world, local_rank):
                      "kernel": f"{dom[0]} pass ({'k_row_hio_p<false,2048>' if dom[0] == 'row' else 'k_col_p16<2048,4>'})",
                      "peak_source": peak_kind,
                      "algorithmic_bytes_per_launch": dom[1], "ms_per_launch": dom[2],
+                     "launch_timing": "pair time: CUDA events around 20 row/column pairs replayed "
+                                      "from one captured graph (the reconstruction's own execution "
+                                      "mode); split between the passes as a replay with an event "
+                                      "after every pass measures",
                      "row_pass_gbs": row_gbs, "col_pass_gbs": col_gbs,
                      "hio_iteration_gbs": iter_gbs, "hio_iteration_frac": iter_gbs / peak},
         "clocks": clk,

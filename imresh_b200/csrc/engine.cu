@@ -942,40 +942,77 @@ int imr_plan_copy_state(imr_plan *P, int what, void *h_dst, void *stream)
     return IMR_SUCCESS;
 }
 
+// One replay of `iters` (row pass, column pass) pairs captured into a graph;
+// with `split`, an event record node after every pass (ev[0..2*iters]),
+// else only before and after the pairs (ev[0], ev[1]).  External records: a
+// plain record inside a capture only orders streams.
+static cudaError_t profile_replay(imr_plan *P, int iters, bool split, cudaStream_t s, std::vector<cudaEvent_t> &ev)
+{
+    const JobDev &J = P->hj;
+    cudaStream_t cs = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return e;
+    cudaGraph_t gr = nullptr;
+    cudaGraphExec_t gx = nullptr;
+    e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        int k = 0;
+        cudaEventRecordWithFlags(ev[k++], cs, cudaEventRecordExternal);
+        for (int i = 0; i < iters; ++i) {
+            if (P->p_rows)
+                P->rk.p_hio<<<P->g_row, P->rk.threads, P->rk.p_smem, cs>>>(P->dj, P->Lrow);
+            else
+                P->rk.hio<<<J.n_row_tiles, P->rk.threads, P->smem_row, cs>>>(P->dj, P->Lrow);
+            if (split) cudaEventRecordWithFlags(ev[k++], cs, cudaEventRecordExternal);
+            if (P->p_cols)
+                P->ck.p_col<<<P->g_col, P->ck.p_threads, P->ck.p_smem, cs>>>(P->dj, P->Lcol);
+            else
+                P->ck.col<<<J.n_col_tiles, P->ck.threads, P->smem_col, cs>>>(P->dj, P->Lcol);
+            if (split || i == iters - 1) cudaEventRecordWithFlags(ev[k++], cs, cudaEventRecordExternal);
+        }
+        const cudaError_t e2 = cudaStreamEndCapture(cs, &gr);
+        e = e2 != cudaSuccess ? e2 : cudaGraphInstantiate(&gx, gr, 0);
+    }
+    if (e == cudaSuccess) e = cudaMemsetAsync(P->st, 0, sizeof(JobState), s);
+    if (e == cudaSuccess) e = cudaGraphLaunch(gx, s);   // warm-up
+    if (e == cudaSuccess) e = cudaGraphLaunch(gx, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (gx) cudaGraphExecDestroy(gx);
+    if (gr) cudaGraphDestroy(gr);
+    cudaStreamDestroy(cs);
+    return e;
+}
+
 int imr_plan_profile(imr_plan *P, int iters, void *stream, float *ms_row, float *ms_col)
 {
     if (!P || iters < 1 || !ms_row || !ms_col) return IMR_ERR_INVALID_VALUE;
     cudaStream_t s = (cudaStream_t)stream;
-    const JobDev &J = P->hj;
-    std::vector<cudaEvent_t> ev(2 * iters + 1);
-    for (auto &e : ev) CK(cudaEventCreate(&e));
-    CK(cudaMemsetAsync(P->st, 0, sizeof(JobState), s));
-    CK(cudaEventRecord(ev[0], s));
-    for (int i = 0; i < iters; ++i) {
-        if (P->p_rows)
-            P->rk.p_hio<<<P->g_row, P->rk.threads, P->rk.p_smem, s>>>(P->dj, P->Lrow);
-        else
-            P->rk.hio<<<J.n_row_tiles, P->rk.threads, P->smem_row, s>>>(P->dj, P->Lrow);
-        CK(cudaEventRecord(ev[2 * i + 1], s));
-        if (P->p_cols)
-            P->ck.p_col<<<P->g_col, P->ck.p_threads, P->ck.p_smem, s>>>(P->dj, P->Lcol);
-        else
-            P->ck.col<<<J.n_col_tiles, P->ck.threads, P->smem_col, s>>>(P->dj, P->Lcol);
-        CK(cudaEventRecord(ev[2 * i + 2], s));
-    }
-    CK(cudaGetLastError());
-    CK(cudaEventSynchronize(ev[2 * iters]));
+    // The pair time comes from a graph of `iters` pairs with no event inside
+    // (kernel after kernel, as a reconstruction runs them: an event between
+    // two kernels drains the GPU and adds that gap to the pass); its split
+    // between the two passes from a replay with an event after every pass.
+    std::vector<cudaEvent_t> ev(2 * iters + 1, nullptr);
+    for (auto &x : ev) CK(cudaEventCreate(&x));
+    cudaError_t e = profile_replay(P, iters, false, s, ev);
+    float pair = 0;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&pair, ev[0], ev[1]);
+    if (e == cudaSuccess) e = profile_replay(P, iters, true, s, ev);
     double tr = 0, tc = 0;
-    for (int i = 0; i < iters; ++i) {
+    for (int i = 0; i < iters && e == cudaSuccess; ++i) {
         float a = 0, b = 0;
-        CK(cudaEventElapsedTime(&a, ev[2 * i], ev[2 * i + 1]));
-        CK(cudaEventElapsedTime(&b, ev[2 * i + 1], ev[2 * i + 2]));
+        e = cudaEventElapsedTime(&a, ev[2 * i], ev[2 * i + 1]);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&b, ev[2 * i + 1], ev[2 * i + 2]);
         tr += a;
         tc += b;
     }
-    for (auto &e : ev) cudaEventDestroy(e);
-    *ms_row = (float)(tr / iters);
-    *ms_col = (float)(tc / iters);
+    for (auto &x : ev) cudaEventDestroy(x);
+    if (e != cudaSuccess) {
+        set_error("imr_plan_profile", e);
+        return IMR_ERR_CUDA;
+    }
+    const double per_pair = (double)pair / iters, frac_row = tr + tc > 0 ? tr / (tr + tc) : 0.5;
+    *ms_row = (float)(per_pair * frac_row);
+    *ms_col = (float)(per_pair * (1.0 - frac_row));
     return IMR_SUCCESS;
 }
 

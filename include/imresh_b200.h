@@ -103,10 +103,16 @@ int imr_plan_launches(imr_plan *plan, long *launches);
  *        2: g_prev (W*H complex64)
  *        3: blurred |g'| of the last cycle (W*H float32) */
 int imr_plan_copy_state(imr_plan *plan, int what, void *h_dst, void *stream);
-/* Times the two passes of one HIO iteration on `stream` with CUDA events:
- * runs `iters` (row pass, column pass) pairs on the plan's current state and
- * returns the mean milliseconds of each pass.  Synchronous.  Leaves the
- * plan's iterate changed; run it after imr_plan_execute, not inside one. */
+/* Times the two passes of one HIO iteration on `stream` with CUDA events,
+ * on the plan's current state: the mean time of a (row pass, column pass)
+ * pair from a captured graph of `iters` pairs with events only before and
+ * after them (kernel after kernel, as a reconstruction runs them), split
+ * between the two passes in the proportion a second replay with an event
+ * after every pass measures (those events drain the GPU between kernels, so
+ * they time the proportion, not the pair).  Each graph is replayed once
+ * untimed first.  Returns the mean milliseconds of each pass.  Synchronous.
+ * Leaves the plan's iterate changed; run it after imr_plan_execute, not
+ * inside one. */
 int imr_plan_profile(imr_plan *plan, int iters, void *stream, float *ms_row_pass,
                      float *ms_col_pass);
 /* Algorithmic HBM bytes of one row pass and one column pass: every image
