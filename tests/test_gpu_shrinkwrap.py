@@ -42,7 +42,10 @@ def _run_gpu(M, p: oracle.SwParams, cuda_defaults=False):
 
 
 @pytest.mark.parametrize("shape", [(64, 64), (256, 256), (128, 384), (192, 512), (2048, 2048),
-                                   (97, 130), (211, 64)])
+                                   (97, 130), (211, 64),
+                                   # column-tiled modulus: 2-column tiles at length 4096, and a
+                                   # last tile of 4 of 16 columns
+                                   (4096, 64), (256, 132)])
 def test_one_cycle_matches_oracle(cuda, shape):
     H, W = shape
     M, _ = data.make_modulus(_spec(W, H), 1)
@@ -55,7 +58,7 @@ def test_one_cycle_matches_oracle(cuda, shape):
     assert errs[0] == pytest.approx(ref.errors[0], rel=1e-4)
 
 
-@pytest.mark.parametrize("shape", [(64, 64), (256, 256), (96, 160)])
+@pytest.mark.parametrize("shape", [(64, 64), (256, 256), (96, 160), (128, 200)])
 def test_five_iterations_match_oracle(cuda, shape):
     """One cycle of five HIO iterations: before HIO's amplification takes
     over (about x2 per iteration on these inputs) the GPU stays within 1e-4
