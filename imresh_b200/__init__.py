@@ -274,7 +274,9 @@ class CResult(C.Structure):
 class CEngineInfo(C.Structure):
     _fields_ = [("pending", C.c_int), ("active", C.c_int), ("done", C.c_int),
                 ("device_bytes_used", C.c_size_t), ("device_bytes_peak", C.c_size_t),
-                ("device_bytes_budget", C.c_size_t), ("launches", C.c_long), ("steps", C.c_long)]
+                ("device_bytes_budget", C.c_size_t), ("launches", C.c_long), ("steps", C.c_long),
+                ("host_launches", C.c_long), ("kernels_per_step", C.c_long), ("graph_builds", C.c_long),
+                ("graph_updates", C.c_long), ("alloc_failures", C.c_long), ("resident", C.c_int)]
 
 
 def _engine_sigs(L):
@@ -291,6 +293,8 @@ def _engine_sigs(L):
     L.imr_engine_checkpoint.argtypes = [vp, C.c_longlong, vp, C.c_size_t]
     L.imr_engine_suspend.argtypes = [vp, C.c_longlong, vp, C.c_size_t]
     L.imr_engine_resume.argtypes = [vp, vp, C.c_size_t, vp]
+    L.imr_engine_cancel.argtypes = [vp, C.c_longlong]
+    L.imr_engine_inject_alloc_failures.argtypes = [vp, C.c_int]
 
 
 class Engine:
@@ -367,6 +371,14 @@ class Engine:
                "imr_engine_resume")
         self._keep[tag] = (buf, out)
         return out
+
+    def cancel(self, tag: int):
+        """Cancel a pending or running request (reported with IMR_ERR_CANCELLED)."""
+        _check(lib().imr_engine_cancel(self._h, tag), "imr_engine_cancel")
+
+    def inject_alloc_failures(self, count: int):
+        """Make the device allocations of the next `count` admissions fail (tests)."""
+        _check(lib().imr_engine_inject_alloc_failures(self._h, count), "imr_engine_inject_alloc_failures")
 
     def info(self) -> dict:
         i = CEngineInfo()

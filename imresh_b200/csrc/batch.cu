@@ -14,6 +14,18 @@
 // ones (stop test met or cycles exhausted, decided on the device) retire and
 // their results are copied out.  Between steps a reconstruction can be saved
 // to host memory and suspended, and resumed later in this or another engine.
+//
+// A step is one CUDA graph: the launches of one cycle of every active
+// reconstruction are captured once and replayed step after step; the graph
+// is rebuilt (re-captured and updated in place where its shape allows) only
+// when the active set changes.  Every kernel skips the items of stopped
+// reconstructions, so a graph stays valid while its reconstructions finish
+// on the device.  The host learns of finished reconstructions from an
+// asynchronous copy of all job states made after every step and read two
+// steps later, so the host never waits for the step it just launched: the
+// GPU always has the next step queued while the host admits, retires and
+// rebuilds.  Results leave through pinned staging and reach the caller's
+// buffer once their copy is known to be complete.
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string.h>
@@ -23,6 +35,8 @@
 #include <deque>
 #include <map>
 #include <vector>
+
+#include <stdio.h>
 
 #include "imresh_b200.h"
 #include "kernels.cuh"
@@ -35,6 +49,13 @@ static double now_ms()
     using namespace std::chrono;
     return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
 }
+
+// Pinned host staging for one result (reused once its copy is complete).
+struct Staging {
+    char *p = nullptr;
+    size_t cap = 0;
+    bool busy = false;
+};
 
 struct EJob {
     int slot = -1;
@@ -50,6 +71,9 @@ struct EJob {
     int cycles_done = 0;
     float last_error = 0.f;
     int status = IMR_SUCCESS;
+    long admit_step = -1;       // its state was set before this step's state copy: older copies are stale
+    long copy_step = -1;        // retiring: its result copy precedes this step's status copy
+    int staging = -1;           // retiring: index of its pinned staging buffer (-1: direct copy)
     std::vector<char> resume;   // snapshot to continue from (empty: a new request)
 };
 
@@ -92,26 +116,47 @@ using namespace imr;
 
 struct imr_engine {
     int dev = 0;
-    cudaStream_t s = nullptr;
+    cudaStream_t s = nullptr;       // the caller's stream: every engine operation is ordered on it
+    cudaStream_t cs = nullptr;      // private stream the step graph is captured on
     cudaMemPool_t pool = nullptr;   // the engine's own pool: freed arenas stay cached for new admissions
     size_t budget = 0, used = 0, peak = 0;
     int max_slots = 0;
     JobDev *dj = nullptr;           // [max_slots]
     JobState *dst = nullptr;        // [max_slots]
-    JobState *hst = nullptr;        // pinned mirror
+    JobState *hst[2] = {nullptr, nullptr};   // pinned copies of dst after steps of each parity
+    cudaEvent_t ev_st[2] = {nullptr, nullptr};
+    long st_step[2] = {-1, -1};     // the step whose state copy each of them receives
+    long synced_step = -1;          // last step whose state copy the host has acted on
     std::vector<int> free_slots;
     std::deque<EJob *> pending;
     std::vector<EJob *> active;
-    std::vector<EJob *> done;
+    std::vector<EJob *> retiring;   // finished on the device, result copy in flight
+    std::deque<EJob *> done;
+    std::vector<Staging> staging;
+    // work lists: device buffers and two pinned staging copies (alternating per rebuild)
     WorkItem *d_items = nullptr;
     size_t items_cap = 0;
     WorkList *d_lists = nullptr;
     size_t lists_cap = 0;
-    WorkItem *h_items = nullptr;   // pinned staging
-    WorkList *h_lists = nullptr;
-    long launches = 0;
+    WorkItem *h_items[2] = {nullptr, nullptr};
+    WorkList *h_lists[2] = {nullptr, nullptr};
+    size_t h_items_cap[2] = {0, 0}, h_lists_cap[2] = {0, 0};
+    cudaEvent_t ev_lists[2] = {nullptr, nullptr};
+    int lists_parity = 0;
+    // the step graph over the active set
+    bool dirty = true;
+    std::vector<EJob *> fresh;      // admitted since the last step: column init before the next graph
+    std::vector<Group> init_groups;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    long kernels_per_step = 0;
+    long launches = 0;              // kernels run (graph kernels count once per step)
+    long host_launches = 0;         // launch calls issued by the host (a graph launch counts once)
+    long graph_builds = 0, graph_updates = 0;
     long steps = 0;
     int sms = 148;
+    int inject_alloc_fail = 0;      // the next admissions whose allocation is made to fail
+    long alloc_failures = 0;
 };
 
 #define CKE(call)                      \
@@ -125,21 +170,40 @@ struct imr_engine {
 
 static int grow(imr_engine *E, size_t n_items, size_t n_lists)
 {
+    if (n_items > E->items_cap || n_lists > E->lists_cap) {
+        // queued steps may still read the old lists
+        CKE(cudaStreamSynchronize(E->s));
+    }
     if (n_items > E->items_cap) {
         size_t cap = std::max(n_items, E->items_cap * 2 + 1024);
         if (E->d_items) cudaFree(E->d_items);
-        if (E->h_items) cudaFreeHost(E->h_items);
+        E->d_items = nullptr;
         CKE(cudaMalloc(&E->d_items, cap * sizeof(WorkItem)));
-        CKE(cudaMallocHost(&E->h_items, cap * sizeof(WorkItem)));
         E->items_cap = cap;
     }
     if (n_lists > E->lists_cap) {
         size_t cap = std::max(n_lists, E->lists_cap * 2 + 256);
         if (E->d_lists) cudaFree(E->d_lists);
-        if (E->h_lists) cudaFreeHost(E->h_lists);
+        E->d_lists = nullptr;
         CKE(cudaMalloc(&E->d_lists, cap * sizeof(WorkList)));
-        CKE(cudaMallocHost(&E->h_lists, cap * sizeof(WorkList)));
         E->lists_cap = cap;
+    }
+    const int q = E->lists_parity;
+    // the staging copy of this parity was last uploaded two rebuilds ago
+    CKE(cudaEventSynchronize(E->ev_lists[q]));
+    if (n_items > E->h_items_cap[q]) {
+        if (E->h_items[q]) cudaFreeHost(E->h_items[q]);
+        E->h_items[q] = nullptr;
+        const size_t cap = std::max(n_items, E->h_items_cap[q] * 2 + 1024);
+        CKE(cudaMallocHost(&E->h_items[q], cap * sizeof(WorkItem)));
+        E->h_items_cap[q] = cap;
+    }
+    if (n_lists > E->h_lists_cap[q]) {
+        if (E->h_lists[q]) cudaFreeHost(E->h_lists[q]);
+        E->h_lists[q] = nullptr;
+        const size_t cap = std::max(n_lists, E->h_lists_cap[q] * 2 + 256);
+        CKE(cudaMallocHost(&E->h_lists[q], cap * sizeof(WorkList)));
+        E->h_lists_cap[q] = cap;
     }
     return IMR_SUCCESS;
 }
@@ -147,20 +211,43 @@ static int grow(imr_engine *E, size_t n_items, size_t n_lists)
 // Loop-kernel grid: enough CTAs to fill the GPU, never more than the items.
 static int loop_grid(const imr_engine *E, int items) { return std::max(1, std::min(items, E->sms * 16)); }
 
-static int admit(imr_engine *E, std::vector<EJob *> &fresh)
+static void finish_now(imr_engine *E, EJob *j, int status)
+{
+    j->status = status;
+    j->t_done = now_ms();
+    E->done.push_back(j);
+}
+
+static int admit(imr_engine *E)
 {
     while (!E->pending.empty() && !E->free_slots.empty()) {
         EJob *j = E->pending.front();
-        if (E->used + j->S.bytes > E->budget && !(E->active.empty() && fresh.empty())) break;
+        const bool idle = E->active.empty() && E->fresh.empty();
+        if (E->used + j->S.bytes > E->budget && !idle) break;
         E->pending.pop_front();
         j->slot = E->free_slots.back();
         E->free_slots.pop_back();
-        cudaError_t e = cudaMallocFromPoolAsync((void **)&j->arena, j->S.bytes, E->pool, E->s);
-        if (e != cudaSuccess) {   // allocation failed: back to the queue, retry later
+        cudaError_t e;
+        if (E->inject_alloc_fail > 0) {   // host-side fault injection: this allocation fails
+            --E->inject_alloc_fail;
+            e = cudaErrorMemoryAllocation;
+        } else {
+            e = cudaMallocFromPoolAsync((void **)&j->arena, j->S.bytes, E->pool, E->s);
+        }
+        if (e != cudaSuccess) {
+            ++E->alloc_failures;
+            cudaGetLastError();
             E->free_slots.push_back(j->slot);
             j->slot = -1;
-            E->pending.push_front(j);
-            cudaGetLastError();
+            j->arena = nullptr;
+            if (idle && E->retiring.empty()) {
+                // nothing running will free memory: the request cannot be served
+                snprintf(g_last_error, sizeof(g_last_error), "engine: %zu device bytes for a %ux%u request not available",
+                         j->S.bytes, j->W, j->H);
+                finish_now(E, j, IMR_ERR_OUT_OF_MEMORY);
+                continue;
+            }
+            E->pending.push_front(j);   // retry once a running reconstruction has retired
             break;
         }
         E->used += j->S.bytes;
@@ -172,26 +259,34 @@ static int admit(imr_engine *E, std::vector<EJob *> &fresh)
             CKE(cudaMemsetAsync(E->dst + j->slot, 0, sizeof(JobState), E->s));
             CKE(cudaMemcpyAsync((void *)j->J.M, j->h_in, (size_t)j->W * j->H * 4, cudaMemcpyHostToDevice, E->s));
             if ((rc = job_modulus_tiles(j->J, E->s))) return rc;
-            if (j->J.Mt) ++E->launches;
-            fresh.push_back(j);
+            if (j->J.Mt) {
+                ++E->launches;
+                ++E->host_launches;
+            }
+            E->fresh.push_back(j);
         } else {   // continue a suspended reconstruction where it stopped
             const SnapHeader *h = (const SnapHeader *)j->resume.data();
             const size_t N = (size_t)j->W * j->H;
             const char *d = j->resume.data() + sizeof(SnapHeader);
             // on the engine's stream, after job_upload's clearing of the mask and
-            // errors; a copy from pageable memory has staged its source on return
+            // errors; synchronised below before the snapshot buffer is released
             CKE(cudaMemcpyAsync(E->dst + j->slot, &h->st, sizeof(JobState), cudaMemcpyHostToDevice, E->s));
             CKE(cudaMemcpyAsync(j->J.X, d, N * 8, cudaMemcpyHostToDevice, E->s));
             CKE(cudaMemcpyAsync(j->J.G, d + N * 8, N * 8, cudaMemcpyHostToDevice, E->s));
             CKE(cudaMemcpyAsync((void *)j->J.M, d + N * 16, N * 4, cudaMemcpyHostToDevice, E->s));
             if ((rc = job_modulus_tiles(j->J, E->s))) return rc;
-            if (j->J.Mt) ++E->launches;
+            if (j->J.Mt) {
+                ++E->launches;
+                ++E->host_launches;
+            }
             CKE(cudaMemcpyAsync(j->J.mask, d + N * 20, N, cudaMemcpyHostToDevice, E->s));
             CKE(cudaMemcpyAsync(j->J.errors, d + N * 21, (size_t)h->n_err * 4, cudaMemcpyHostToDevice, E->s));
             CKE(cudaStreamSynchronize(E->s));
             std::vector<char>().swap(j->resume);
         }
+        j->admit_step = E->steps;   // the slot's previous state is in every older state copy
         E->active.push_back(j);
+        E->dirty = true;
     }
     return IMR_SUCCESS;
 }
@@ -236,52 +331,13 @@ static void build_groups(const std::vector<EJob *> &jobs, bool rows, std::vector
     }
 }
 
-static int launch_step(imr_engine *E, const std::vector<EJob *> &fresh)
+// The launches of one cycle of every job in the groups, on stream s (a
+// capturing stream when the step graph is built).  Returns the kernel count.
+static int launch_cycle(imr_engine *E, cudaStream_t s, const WorkList *L, std::vector<Group> &rowg,
+                        std::vector<Group> &colg, int vb_base, size_t n_vb, long *kernels)
 {
-    cudaStream_t s = E->s;
-    // --- column init of newly admitted jobs
-    std::vector<Group> init_groups, rowg, colg;
-    build_groups(fresh, false, init_groups);
-    std::vector<EJob *> live;
-    for (EJob *j : E->active) live.push_back(j);
-    build_groups(live, true, rowg);
-    build_groups(live, false, colg);
-    // vertical-blur items: every live job
-    std::vector<WorkItem> vb;
-    for (EJob *j : live)
-        for (int t = 0; t < j->J.n_vb_tiles; ++t) vb.push_back(WorkItem{j->slot, t});
-
-    size_t n_items = vb.size(), n_lists = 1;
-    for (auto *G : {&init_groups, &rowg, &colg})
-        for (auto &g : *G) {
-            n_items += g.items.size();
-            n_lists += 1 + g.hio_count.size();
-        }
-    int rc = grow(E, n_items, n_lists);
-    if (rc) return rc;
-    size_t ip = 0, lp = 0;
-    auto put = [&](const std::vector<WorkItem> &items, const std::vector<int> &counts, int &base) {
-        const WorkItem *dptr = E->d_items + ip;
-        memcpy(E->h_items + ip, items.data(), items.size() * sizeof(WorkItem));
-        base = (int)lp;
-        E->h_lists[lp++] = WorkList{dptr, (int)items.size()};
-        for (int c : counts) E->h_lists[lp++] = WorkList{dptr, c};
-        ip += items.size();
-    };
-    int vb_base = 0;
-    put(vb, {}, vb_base);
-    for (auto *G : {&init_groups, &rowg, &colg})
-        for (auto &g : *G) put(g.items, g.hio_count, g.list_base);
-    CKE(cudaMemcpyAsync(E->d_items, E->h_items, ip * sizeof(WorkItem), cudaMemcpyHostToDevice, s));
-    CKE(cudaMemcpyAsync(E->d_lists, E->h_lists, lp * sizeof(WorkList), cudaMemcpyHostToDevice, s));
-    const WorkList *L = E->d_lists;
-
-    for (auto &g : init_groups) {
-        g.ck.init<<<loop_grid(E, (int)g.items.size()), g.ck.threads, g.ck.smem ? g.ck.smem : g.smem, s>>>(
-            E->dj, L + g.list_base);
-        ++E->launches;
-    }
-    // --- one shrink-wrap cycle of every live job
+    long k = 0;
+    int rc;
     for (auto &g : rowg) {
         if (g.pipelined) {
             if ((rc = launch_finish(g.rk, (int)g.items.size(), g.smem_fin, s, E->dj, L + g.list_base, nullptr)))
@@ -290,11 +346,11 @@ static int launch_step(imr_engine *E, const std::vector<EJob *> &fresh)
             g.rk.finish<<<loop_grid(E, (int)g.items.size()), g.rk.threads, g.smem_fin, s>>>(E->dj, L + g.list_base,
                                                                                          nullptr);
         }
-        ++E->launches;
+        ++k;
     }
-    if (!vb.empty()) {
-        k_vblur<<<loop_grid(E, (int)vb.size()), kVbThreads, 0, s>>>(E->dj, L + vb_base);
-        ++E->launches;
+    if (n_vb) {
+        k_vblur<<<loop_grid(E, (int)n_vb), kVbThreads, 0, s>>>(E->dj, L + vb_base);
+        ++k;
     }
     int max_hio = 0;
     for (auto &g : rowg) max_hio = std::max(max_hio, (int)g.hio_count.size());
@@ -304,13 +360,13 @@ static int launch_step(imr_engine *E, const std::vector<EJob *> &fresh)
             const WorkList *Li = L + g.list_base + 1 + i;
             const int n = g.hio_count[i];
             if (g.pipelined) {
-                auto k = i == 0 ? g.rk.p_hio_first : g.rk.p_hio;
+                auto kf = i == 0 ? g.rk.p_hio_first : g.rk.p_hio;
                 const int sm = i == 0 ? g.rk.p_smem_first : g.rk.p_smem;
-                k<<<persistent_grid((const void *)k, g.rk.threads, sm, n), g.rk.threads, sm, s>>>(E->dj, Li);
+                kf<<<persistent_grid((const void *)kf, g.rk.threads, sm, n), g.rk.threads, sm, s>>>(E->dj, Li);
             } else {
                 (i == 0 ? g.rk.hio_first : g.rk.hio)<<<loop_grid(E, n), g.rk.threads, g.smem, s>>>(E->dj, Li);
             }
-            ++E->launches;
+            ++k;
         }
         for (auto &g : colg) {
             if (i >= (int)g.hio_count.size()) continue;
@@ -321,44 +377,198 @@ static int launch_step(imr_engine *E, const std::vector<EJob *> &fresh)
                              g.ck.p_threads, g.ck.p_smem, s>>>(E->dj, Li);
             else
                 g.ck.col<<<loop_grid(E, n), g.ck.threads, g.smem, s>>>(E->dj, Li);
-            ++E->launches;
+            ++k;
         }
     }
-    CKE(cudaGetLastError());
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error("engine kernel launch", e);
+        return IMR_ERR_CUDA;
+    }
+    *kernels = k;
     return IMR_SUCCESS;
 }
 
-static int retire(imr_engine *E)
+// Rebuild the work lists of the active set and the newly admitted jobs'
+// column init, upload them (stream-ordered after the queued steps, which
+// still read the previous lists), and re-capture the step graph.
+static int rebuild(imr_engine *E)
 {
-    CKE(cudaMemcpyAsync(E->hst, E->dst, sizeof(JobState) * E->max_slots, cudaMemcpyDeviceToHost, E->s));
-    CKE(cudaStreamSynchronize(E->s));
-    std::vector<EJob *> keep, out;
-    for (EJob *j : E->active) {
-        const JobState &st = E->hst[j->slot];
-        if (st.stop || st.err) {
-            j->cycles_done = st.cycles_done;
-            j->last_error = st.last_error;
-            j->status = st.err ? IMR_ERR_DEVICE_TIMEOUT : IMR_SUCCESS;
-            CKE(cudaMemcpyAsync(j->h_out, j->J.out, (size_t)j->W * j->H * 4, cudaMemcpyDeviceToHost, E->s));
-            CKE(cudaFreeAsync(j->arena, E->s));
-            out.push_back(j);
-        } else {
-            keep.push_back(j);
+    std::vector<Group> rowg, colg;
+    build_groups(E->fresh, false, E->init_groups);
+    build_groups(E->active, true, rowg);
+    build_groups(E->active, false, colg);
+    std::vector<WorkItem> vb;
+    for (EJob *j : E->active)
+        for (int t = 0; t < j->J.n_vb_tiles; ++t) vb.push_back(WorkItem{j->slot, t});
+    size_t n_items = vb.size(), n_lists = 1;
+    for (auto *G : {&E->init_groups, &rowg, &colg})
+        for (auto &g : *G) {
+            n_items += g.items.size();
+            n_lists += 1 + g.hio_count.size();
         }
+    int rc = grow(E, n_items, n_lists);
+    if (rc) return rc;
+    const int q = E->lists_parity;
+    WorkItem *hi = E->h_items[q];
+    WorkList *hl = E->h_lists[q];
+    size_t ip = 0, lp = 0;
+    auto put = [&](const std::vector<WorkItem> &items, const std::vector<int> &counts, int &base) {
+        const WorkItem *dptr = E->d_items + ip;
+        if (!items.empty()) memcpy(hi + ip, items.data(), items.size() * sizeof(WorkItem));
+        base = (int)lp;
+        hl[lp++] = WorkList{dptr, (int)items.size()};
+        for (int c : counts) hl[lp++] = WorkList{dptr, c};
+        ip += items.size();
+    };
+    int vb_base = 0;
+    put(vb, {}, vb_base);
+    for (auto *G : {&E->init_groups, &rowg, &colg})
+        for (auto &g : *G) put(g.items, g.hio_count, g.list_base);
+    if (ip) CKE(cudaMemcpyAsync(E->d_items, hi, ip * sizeof(WorkItem), cudaMemcpyHostToDevice, E->s));
+    CKE(cudaMemcpyAsync(E->d_lists, hl, lp * sizeof(WorkList), cudaMemcpyHostToDevice, E->s));
+    CKE(cudaEventRecord(E->ev_lists[q], E->s));
+    E->lists_parity ^= 1;
+
+    // capture one cycle of every active job
+    cudaGraph_t g = nullptr;
+    long kernels = 0;
+    CKE(cudaStreamBeginCapture(E->cs, cudaStreamCaptureModeThreadLocal));
+    rc = launch_cycle(E, E->cs, E->d_lists, rowg, colg, vb_base, vb.size(), &kernels);
+    const cudaError_t ec = cudaStreamEndCapture(E->cs, &g);
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    CKE(ec);
+    bool updated = false;
+    if (E->gexec) {
+        cudaGraphExecUpdateResultInfo info;
+        if (cudaGraphExecUpdate(E->gexec, g, &info) == cudaSuccess) {
+            updated = true;
+        } else {
+            cudaGetLastError();
+            cudaGraphExecDestroy(E->gexec);
+            E->gexec = nullptr;
+        }
+    }
+    if (!updated) {
+        const cudaError_t e = cudaGraphInstantiate(&E->gexec, g, 0);
+        if (e != cudaSuccess) {
+            cudaGraphDestroy(g);
+            set_error("engine step graph", e);
+            return IMR_ERR_CUDA;
+        }
+    }
+    if (E->graph) cudaGraphDestroy(E->graph);
+    E->graph = g;
+    E->kernels_per_step = kernels;
+    ++(updated ? E->graph_updates : E->graph_builds);
+    E->dirty = false;
+    return IMR_SUCCESS;
+}
+
+static int stage_index(imr_engine *E, size_t bytes)
+{
+    for (size_t i = 0; i < E->staging.size(); ++i)
+        if (!E->staging[i].busy && E->staging[i].cap >= bytes) return (int)i;
+    Staging st;
+    const size_t cap = std::max(bytes, (size_t)1 << 20);
+    if (cudaMallocHost(&st.p, cap) != cudaSuccess) {
+        cudaGetLastError();
+        return -2;
+    }
+    st.cap = cap;
+    E->staging.push_back(st);
+    return (int)E->staging.size() - 1;
+}
+
+// Retire the jobs that had stopped (or failed) by the end of step m, whose
+// states are in hst: copy their results out (stream-ordered, before the next
+// step), release their device memory and slots.
+static int observe(imr_engine *E, const JobState *hs, long m)
+{
+    E->synced_step = m;
+    // result copies issued before step m's state copy are complete
+    for (size_t i = 0; i < E->retiring.size();) {
+        EJob *j = E->retiring[i];
+        if (j->copy_step >= 0 && j->copy_step <= m) {
+            const size_t b = (size_t)j->W * j->H * 4;
+            if (j->staging >= 0) {
+                memcpy(j->h_out, E->staging[j->staging].p, b);
+                E->staging[j->staging].busy = false;
+            }
+            finish_now(E, j, j->status);
+            E->retiring.erase(E->retiring.begin() + i);
+        } else {
+            ++i;
+        }
+    }
+    if (!hs) return IMR_SUCCESS;
+    std::vector<EJob *> keep;
+    for (EJob *j : E->active) {
+        const JobState &st = hs[j->slot];
+        if (m < j->admit_step || !(st.stop || st.err)) {
+            keep.push_back(j);
+            continue;
+        }
+        j->cycles_done = st.cycles_done;
+        j->last_error = st.last_error;
+        j->status = st.err ? IMR_ERR_DEVICE_TIMEOUT : IMR_SUCCESS;
+        const size_t b = (size_t)j->W * j->H * 4;
+        cudaPointerAttributes pa;
+        const bool pinned = cudaPointerGetAttributes(&pa, j->h_out) == cudaSuccess &&
+                            (pa.type == cudaMemoryTypeHost || pa.type == cudaMemoryTypeManaged);
+        cudaGetLastError();
+        j->staging = pinned ? -1 : stage_index(E, b);
+        if (j->staging == -2) {
+            set_error("engine result staging", cudaErrorMemoryAllocation);
+            return IMR_ERR_OUT_OF_MEMORY;
+        }
+        void *dst = j->staging >= 0 ? (void *)E->staging[j->staging].p : (void *)j->h_out;
+        if (j->staging >= 0) E->staging[j->staging].busy = true;
+        CKE(cudaMemcpyAsync(dst, j->J.out, b, cudaMemcpyDeviceToHost, E->s));
+        CKE(cudaFreeAsync(j->arena, E->s));
+        j->arena = nullptr;
+        j->copy_step = E->steps;   // the copy precedes the state copy of the next step launched
+        E->used -= j->S.bytes;
+        E->free_slots.push_back(j->slot);
+        E->retiring.push_back(j);
+        E->dirty = true;
     }
     E->active.swap(keep);
-    if (!out.empty()) {
-        CKE(cudaStreamSynchronize(E->s));
-        const double t = now_ms();
-        for (EJob *j : out) {
-            j->t_done = t;
-            E->used -= j->S.bytes;
-            E->free_slots.push_back(j->slot);
-            j->arena = nullptr;
-            E->done.push_back(j);
-        }
+    return IMR_SUCCESS;
+}
+
+// Act on the newest state copy that has already landed, without waiting
+// (imr_engine_poll between steps).
+static int reap(imr_engine *E)
+{
+    for (int pass = 0; pass < 2; ++pass) {
+        int q = E->st_step[0] < E->st_step[1] ? 0 : 1;   // older first
+        if (pass == 1) q ^= 1;
+        const long m = E->st_step[q];
+        if (m <= E->synced_step) continue;
+        const cudaError_t e = cudaEventQuery(E->ev_st[q]);
+        if (e == cudaErrorNotReady) break;
+        CKE(e);
+        if (int rc = observe(E, E->hst[q], m)) return rc;
     }
     return IMR_SUCCESS;
+}
+
+// Wait for everything queued and hand every retiring result to the caller.
+static int drain(imr_engine *E)
+{
+    CKE(cudaStreamSynchronize(E->s));
+    return observe(E, nullptr, E->steps);
+}
+
+static EJob *find_active(imr_engine *E, long long tag)
+{
+    for (EJob *j : E->active)
+        if (j->tag == tag) return j;
+    return nullptr;
 }
 
 extern "C" {
@@ -400,7 +610,12 @@ int imr_engine_create(imr_engine **out, size_t device_bytes, int max_jobs, void 
     E->max_slots = max_jobs;
     cudaError_t e = cudaMalloc(&E->dj, sizeof(JobDev) * max_jobs);
     if (e == cudaSuccess) e = cudaMalloc(&E->dst, sizeof(JobState) * max_jobs);
-    if (e == cudaSuccess) e = cudaMallocHost(&E->hst, sizeof(JobState) * max_jobs);
+    for (int q = 0; q < 2 && e == cudaSuccess; ++q) {
+        e = cudaMallocHost(&E->hst[q], sizeof(JobState) * max_jobs);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&E->ev_st[q], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&E->ev_lists[q], cudaEventDisableTiming);
+    }
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&E->cs, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMemset(E->dst, 0, sizeof(JobState) * max_jobs);
     if (e != cudaSuccess) {
         set_error("engine create", e);
@@ -436,22 +651,49 @@ int imr_engine_submit(imr_engine *E, const float *h_modulus, float *h_out, unsig
 int imr_engine_step(imr_engine *E)
 {
     if (!E) return IMR_ERR_INVALID_VALUE;
-    std::vector<EJob *> fresh;
-    int rc = admit(E, fresh);
-    if (rc) return rc;
-    if (E->active.empty()) return IMR_SUCCESS;
-    if ((rc = launch_step(E, fresh))) return rc;
+    int rc;
+    const long n = E->steps;
+    if (n >= 2 && n - 2 > E->synced_step) {   // the state after step n - 2 (copied into hst[n & 1])
+        const int q = (int)(n & 1);
+        CKE(cudaEventSynchronize(E->ev_st[q]));
+        if ((rc = observe(E, E->hst[q], n - 2))) return rc;
+    }
+    if ((rc = admit(E))) return rc;
+    if (E->active.empty()) {   // nothing to run: hand over what is still in flight
+        E->fresh.clear();
+        return E->retiring.empty() ? IMR_SUCCESS : drain(E);
+    }
+    if (E->dirty && (rc = rebuild(E))) return rc;
+    // column init of the newly admitted jobs, then one cycle of every active job
+    const WorkList *L = E->d_lists;
+    for (auto &g : E->init_groups) {
+        g.ck.init<<<loop_grid(E, (int)g.items.size()), g.ck.threads, g.ck.smem ? g.ck.smem : g.smem, E->s>>>(
+            E->dj, L + g.list_base);
+        ++E->launches;
+        ++E->host_launches;
+    }
+    CKE(cudaGetLastError());
+    E->init_groups.clear();
+    E->fresh.clear();
+    CKE(cudaGraphLaunch(E->gexec, E->s));
+    ++E->host_launches;
+    E->launches += E->kernels_per_step;
+    const int q = (int)(n & 1);
+    CKE(cudaMemcpyAsync(E->hst[q], E->dst, sizeof(JobState) * E->max_slots, cudaMemcpyDeviceToHost, E->s));
+    CKE(cudaEventRecord(E->ev_st[q], E->s));
+    E->st_step[q] = n;
     ++E->steps;
-    return retire(E);
+    return IMR_SUCCESS;
 }
 
 int imr_engine_poll(imr_engine *E, imr_result *results, int max_results, int *n_results)
 {
     if (!E || !n_results || (max_results > 0 && !results)) return IMR_ERR_INVALID_VALUE;
+    if (int rc = reap(E)) return rc;
     int n = 0;
     while (n < max_results && !E->done.empty()) {
         EJob *j = E->done.front();
-        E->done.erase(E->done.begin());
+        E->done.pop_front();
         imr_result &r = results[n++];
         r.tag = j->tag;
         r.width = j->W;
@@ -469,18 +711,45 @@ int imr_engine_poll(imr_engine *E, imr_result *results, int max_results, int *n_
 int imr_engine_run(imr_engine *E)
 {
     if (!E) return IMR_ERR_INVALID_VALUE;
-    while (!E->pending.empty() || !E->active.empty()) {
+    while (!E->pending.empty() || !E->active.empty() || !E->retiring.empty()) {
         int rc = imr_engine_step(E);
         if (rc) return rc;
     }
     return IMR_SUCCESS;
 }
 
-static EJob *find_active(imr_engine *E, long long tag)
+int imr_engine_cancel(imr_engine *E, long long tag)
 {
-    for (EJob *j : E->active)
-        if (j->tag == tag) return j;
-    return nullptr;
+    if (!E) return IMR_ERR_INVALID_VALUE;
+    for (auto it = E->pending.begin(); it != E->pending.end(); ++it)
+        if ((*it)->tag == tag) {
+            EJob *j = *it;
+            E->pending.erase(it);
+            finish_now(E, j, IMR_ERR_CANCELLED);
+            return IMR_SUCCESS;
+        }
+    EJob *j = find_active(E, tag);
+    if (!j) {
+        snprintf(g_last_error, sizeof(g_last_error), "engine: no pending or running request with tag %lld", tag);
+        return IMR_ERR_INVALID_VALUE;
+    }
+    // steps already queued may still run it: its memory is released after them
+    E->active.erase(std::find(E->active.begin(), E->active.end(), j));
+    E->fresh.erase(std::remove(E->fresh.begin(), E->fresh.end(), j), E->fresh.end());
+    CKE(cudaFreeAsync(j->arena, E->s));
+    j->arena = nullptr;
+    E->used -= j->S.bytes;
+    E->free_slots.push_back(j->slot);
+    E->dirty = true;
+    finish_now(E, j, IMR_ERR_CANCELLED);
+    return IMR_SUCCESS;
+}
+
+int imr_engine_inject_alloc_failures(imr_engine *E, int count)
+{
+    if (!E || count < 0) return IMR_ERR_INVALID_VALUE;
+    E->inject_alloc_fail = count;
+    return IMR_SUCCESS;
 }
 
 int imr_engine_snapshot_size(imr_engine *E, long long tag, size_t *bytes)
@@ -500,7 +769,7 @@ int imr_engine_checkpoint(imr_engine *E, long long tag, void *h_buf, size_t cap)
     const unsigned n_err = (unsigned)j->J.n_cycles + 1;
     const size_t bytes = snap_bytes(j->W, j->H, n_err), N = (size_t)j->W * j->H;
     if (cap < bytes) return IMR_ERR_INVALID_VALUE;
-    CKE(cudaStreamSynchronize(E->s));   // between steps the device state is at rest
+    CKE(cudaStreamSynchronize(E->s));   // the device state at rest after the queued steps
     SnapHeader h;
     memset(&h, 0, sizeof(h));
     memcpy(h.magic, kSnapMagic, 8);
@@ -511,6 +780,10 @@ int imr_engine_checkpoint(imr_engine *E, long long tag, void *h_buf, size_t cap)
     h.n_err = n_err;
     h.bytes = bytes;
     CKE(cudaMemcpy(&h.st, E->dst + j->slot, sizeof(JobState), cudaMemcpyDeviceToHost));
+    if (h.st.stop || h.st.err) {   // finished on the device: its result is on the way, nothing to save
+        snprintf(g_last_error, sizeof(g_last_error), "engine: request %lld has already finished", tag);
+        return IMR_ERR_INVALID_VALUE;
+    }
     char *d = (char *)h_buf;
     memcpy(d, &h, sizeof(h));
     d += sizeof(h);
@@ -528,10 +801,12 @@ int imr_engine_suspend(imr_engine *E, long long tag, void *h_buf, size_t cap)
     if (rc) return rc;
     EJob *j = find_active(E, tag);
     E->active.erase(std::find(E->active.begin(), E->active.end(), j));
+    E->fresh.erase(std::remove(E->fresh.begin(), E->fresh.end(), j), E->fresh.end());
     CKE(cudaFreeAsync(j->arena, E->s));
     CKE(cudaStreamSynchronize(E->s));
     E->used -= j->S.bytes;
     E->free_slots.push_back(j->slot);
+    E->dirty = true;
     delete j;
     return IMR_SUCCESS;
 }
@@ -565,13 +840,19 @@ int imr_engine_stats(imr_engine *E, imr_engine_info *st)
 {
     if (!E || !st) return IMR_ERR_INVALID_VALUE;
     st->pending = (int)E->pending.size();
-    st->active = (int)E->active.size();
+    st->active = (int)(E->active.size() + E->retiring.size());
     st->done = (int)E->done.size();
     st->device_bytes_used = E->used;
     st->device_bytes_peak = E->peak;
     st->device_bytes_budget = E->budget;
     st->launches = E->launches;
     st->steps = E->steps;
+    st->host_launches = E->host_launches;
+    st->kernels_per_step = E->kernels_per_step;
+    st->graph_builds = E->graph_builds;
+    st->graph_updates = E->graph_updates;
+    st->alloc_failures = E->alloc_failures;
+    st->resident = (int)E->active.size();
     return IMR_SUCCESS;
 }
 
@@ -580,22 +861,30 @@ int imr_engine_destroy(imr_engine *E)
     if (!E) return IMR_SUCCESS;
     cudaStreamSynchronize(E->s);
     for (EJob *j : E->active) {
-        if (j->arena) cudaFree(j->arena);
+        if (j->arena) cudaFreeAsync(j->arena, E->s);
         delete j;
     }
+    for (EJob *j : E->retiring) delete j;
     for (EJob *j : E->pending) delete j;
     for (EJob *j : E->done) delete j;
+    cudaStreamSynchronize(E->s);
+    if (E->gexec) cudaGraphExecDestroy(E->gexec);
+    if (E->graph) cudaGraphDestroy(E->graph);
     if (E->dj) cudaFree(E->dj);
     if (E->dst) cudaFree(E->dst);
-    if (E->hst) cudaFreeHost(E->hst);
-    if (E->d_items) cudaFree(E->d_items);
-    if (E->h_items) cudaFreeHost(E->h_items);
-    if (E->d_lists) cudaFree(E->d_lists);
-    if (E->h_lists) cudaFreeHost(E->h_lists);
-    if (E->pool) {
-        cudaStreamSynchronize(E->s);
-        cudaMemPoolDestroy(E->pool);
+    for (int q = 0; q < 2; ++q) {
+        if (E->hst[q]) cudaFreeHost(E->hst[q]);
+        if (E->h_items[q]) cudaFreeHost(E->h_items[q]);
+        if (E->h_lists[q]) cudaFreeHost(E->h_lists[q]);
+        if (E->ev_st[q]) cudaEventDestroy(E->ev_st[q]);
+        if (E->ev_lists[q]) cudaEventDestroy(E->ev_lists[q]);
     }
+    for (auto &st : E->staging)
+        if (st.p) cudaFreeHost(st.p);
+    if (E->d_items) cudaFree(E->d_items);
+    if (E->d_lists) cudaFree(E->d_lists);
+    if (E->cs) cudaStreamDestroy(E->cs);
+    if (E->pool) cudaMemPoolDestroy(E->pool);
     delete E;
     return IMR_SUCCESS;
 }

@@ -741,6 +741,7 @@ const char *imr_status_string(int s)
     case IMR_ERR_NOT_INITIALIZED: return "not initialised";
     case IMR_ERR_QUEUE: return "task queue error";
     case IMR_ERR_DEVICE_TIMEOUT: return "device-side wait timed out";
+    case IMR_ERR_CANCELLED: return "cancelled";
     default: return "unknown status";
     }
 }
@@ -1022,6 +1023,31 @@ int imr_plan_pass_bytes(imr_plan *P, double *row_bytes, double *col_bytes)
     const double N = (double)P->W * P->H;
     *row_bytes = 33.0 * N;
     *col_bytes = 20.0 * N;
+    return IMR_SUCCESS;
+}
+
+int imr_plan_set_wait_limit(imr_plan *P, unsigned long long limit_ns)
+{
+    if (!P) return IMR_ERR_INVALID_VALUE;
+    P->hj.wait_ns = limit_ns;
+    // the captured graphs read the job description from device memory: no re-capture
+    CK(cudaMemcpy(P->dj, &P->hj, sizeof(JobDev), cudaMemcpyHostToDevice));
+    return IMR_SUCCESS;
+}
+
+int imr_bounded_wait_check(unsigned long long limit_ns, unsigned long long *elapsed_ns, void *stream)
+{
+    cudaStream_t s = (cudaStream_t)stream;
+    k_wait_probe<<<1, 32, 0, s>>>(limit_ns);
+    CK(cudaGetLastError());
+    unsigned long long r[2] = {0, 0};
+    CK(cudaMemcpyFromSymbolAsync(r, g_wait_probe, sizeof(r), 0, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (elapsed_ns) *elapsed_ns = r[1];
+    if (r[0] == 0) {
+        snprintf(g_last_error, sizeof(g_last_error), "bounded wait gave up after %llu ns", r[1]);
+        return IMR_ERR_DEVICE_TIMEOUT;
+    }
     return IMR_SUCCESS;
 }
 

@@ -83,6 +83,7 @@ struct alignas(64) JobDev {
     int rpc;                // rows per row-pass CTA
     int cpc;                // columns per column-pass CTA
     int n_row_tiles, n_col_tiles, n_vb_tiles, vb_tiles_x;
+    unsigned long long wait_ns;   // limit of each bounded copy wait (0: kWaitNs, 0.5 s)
 };
 
 // One unit of work: job index and tile (row group / column group) index.

@@ -753,6 +753,26 @@ static __global__ void __launch_bounds__(256) k_hio_error(const float2 *d, const
     }
 }
 
+// Self-check of the bounded wait every pipelined pass relies on: one thread
+// waits on an mbarrier whose transaction nothing will complete (an expected
+// 16 bytes that no copy delivers), so the wait must give up after limit_ns
+// and report it; no copy is in flight, so returning is safe.
+// g_wait_probe = {completed (1) or gave up (0), nanoseconds waited}.
+static __device__ unsigned long long g_wait_probe[2];
+static __global__ void k_wait_probe(unsigned long long limit_ns)
+{
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x != 0) return;
+    mbar_init(&bar, 1);
+    mbar_fence_init();
+    mbar_arrive_expect_tx(&bar, 16u);
+    const uint64_t t0 = global_ns();
+    const bool ok = mbar_wait(&bar, 0u, limit_ns);
+    g_wait_probe[1] = global_ns() - t0;
+    g_wait_probe[0] = ok ? 1ull : 0ull;
+    mbar_inval(&bar);
+}
+
 // Global max of a float array (vectorMax; cudaVectorReduce.cu:229-239):
 // signed floats ordered through an order-preserving integer key.
 __device__ __forceinline__ unsigned f2key(float f)
@@ -1749,11 +1769,13 @@ __global__ void __launch_bounds__(rrow_threads(N), prow_min_blocks(FIRST, FIX, N
         const int kit = FIX ? st->cycle : 0;
         const bool fin = FIX && kit >= J.n_cycles;
         const bool tested = FIX && (J.target > 0.f || fin);
-        const bool landed = mbar_wait(&bars[s], (uint32_t)((k >> 1) & 1));
+        const bool landed = mbar_wait(&bars[s], (uint32_t)((k >> 1) & 1), J.wait_ns);
         if (__syncthreads_or(!landed)) {
             if (threadIdx.x == 0) {
                 atomicExch(&st->err, 1);
-                if (nxt < n_items) mbar_wait(&bars[s ^ 1], (uint32_t)(((k + 1) >> 1) & 1));
+                // the copies still in flight (this item's, the next item's) land before the CTA exits
+                mbar_wait(&bars[s], (uint32_t)((k >> 1) & 1), kDrainNs);
+                if (nxt < n_items) mbar_wait(&bars[s ^ 1], (uint32_t)(((k + 1) >> 1) & 1), kDrainNs);
             }
             return;
         }
@@ -1878,11 +1900,13 @@ __global__ void __launch_bounds__(rrow_threads(N)) k_row_finish_p(const JobDev *
         const int K = J.ntaps[c];
         if (threadIdx.x < kTapStride) wsm[threadIdx.x] = J.weights[(size_t)c * kTapStride + threadIdx.x];
         if (wi.tile == 0 && threadIdx.x == 0) st->max_bits = 0u;
-        const bool landed = mbar_wait(&bars[s], (uint32_t)((k >> 1) & 1));
+        const bool landed = mbar_wait(&bars[s], (uint32_t)((k >> 1) & 1), J.wait_ns);
         if (__syncthreads_or(!landed)) {
             if (threadIdx.x == 0) {
                 atomicExch(&st->err, 1);
-                if (nxt < n_items) mbar_wait(&bars[s ^ 1], (uint32_t)(((k + 1) >> 1) & 1));
+                // the copies still in flight (this item's, the next item's) land before the CTA exits
+                mbar_wait(&bars[s], (uint32_t)((k >> 1) & 1), kDrainNs);
+                if (nxt < n_items) mbar_wait(&bars[s ^ 1], (uint32_t)(((k + 1) >> 1) & 1), kDrainNs);
             }
             return;
         }
@@ -2011,11 +2035,13 @@ __global__ void __launch_bounds__(rcol_threads(N)) k_col_p(const JobDev *jobs, c
         }
         const WorkItem wi = walk.at(item);
         const JobDev &J = jobs[wi.job];
-        const bool landed = mbar_wait(&bars[s], (uint32_t)((k >> 1) & 1));
+        const bool landed = mbar_wait(&bars[s], (uint32_t)((k >> 1) & 1), J.wait_ns);
         if (__syncthreads_or(!landed)) {
             if (threadIdx.x == 0) {
                 atomicExch(&J.st->err, 1);
-                if (nxt < n_items) mbar_wait(&bars[s ^ 1], (uint32_t)(((k + 1) >> 1) & 1));
+                // the copies still in flight (this tile's, the next tile's) land before the CTA exits
+                mbar_wait(&bars[s], (uint32_t)((k >> 1) & 1), kDrainNs);
+                if (nxt < n_items) mbar_wait(&bars[s ^ 1], (uint32_t)(((k + 1) >> 1) & 1), kDrainNs);
                 bulk_wait0();
             }
             return;
@@ -2157,13 +2183,14 @@ k_col_p16(const JobDev *jobs, const WorkList *L)
 #pragma unroll
             for (int m = 0; m < V; ++m) mod[m] = ok ? __ldg(J.M + (size_t)(l + m * Q) * W + x) : 0.f;
         }
-        const bool landed = mbar_wait(&bars[s], (uint32_t)((k / NST) & 1));
+        const bool landed = mbar_wait(&bars[s], (uint32_t)((k / NST) & 1), J.wait_ns);
         if (__syncthreads_or(!landed)) {
             if (threadIdx.x == 0) {
                 atomicExch(&J.st->err, 1);
-                for (int d = 1; d < NST - 1; ++d) {   // tiles already requested beyond this one
+                // this tile and the tiles already requested beyond it land before the CTA exits
+                for (int d = 0; d < NST - 1; ++d) {
                     const int t = (k + d) % NST;
-                    if (s_item[t] < n_items) mbar_wait(&bars[t], (uint32_t)(((k + d) / NST) & 1));
+                    if (d == 0 || s_item[t] < n_items) mbar_wait(&bars[t], (uint32_t)(((k + d) / NST) & 1), kDrainNs);
                 }
                 bulk_wait0();
             }

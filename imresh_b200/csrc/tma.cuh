@@ -3,9 +3,13 @@
 // Only CTA-local loads are used: cp.async.bulk (1D, contiguous rows) and
 // cp.async.bulk.tensor.2d (column tiles through a CUtensorMap), each
 // completing on an mbarrier with a transaction byte count.  No cluster
-// multicast is used anywhere.  Every wait is bounded: after kWaitLimit
-// unsuccessful polls the caller records an error and carries on, so a copy
-// that never lands cannot hang the GPU.
+// multicast is used anywhere.  Every wait is bounded by %globaltimer: a wait
+// that runs past its limit returns false, the caller records an error in the
+// job state and returns, so a copy that never lands cannot hang the GPU.  The
+// limit of a job's waits is JobDev::wait_ns (0: kWaitNs).  A CTA that gave up
+// first waits, bounded by kWaitNs, for every copy it still has in flight
+// (kDrainNs), so no copy can land in the shared memory of an exited CTA even
+// when a short limit made it give up early.
 #pragma once
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -13,7 +17,8 @@
 
 namespace imr {
 
-constexpr uint64_t kWaitNs = 500000000ull;   // give up on a copy after 0.5 s
+constexpr uint64_t kWaitNs = 500000000ull;   // default: give up on a copy after 0.5 s
+constexpr uint64_t kDrainNs = kWaitNs;       // bound of the in-flight drain after giving up
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
 {
@@ -64,14 +69,21 @@ __device__ __forceinline__ uint64_t global_ns()
     return t;
 }
 
-// Bounded wait for the phase with the given parity; false after kWaitNs.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+// Bounded wait for the phase with the given parity; false once limit_ns
+// have passed without it (limit_ns == 0: kWaitNs).
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint64_t limit_ns = kWaitNs)
 {
     if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t lim = limit_ns ? limit_ns : kWaitNs;
     const uint64_t t0 = global_ns();
     while (!mbar_try_wait(bar, parity))
-        if (global_ns() - t0 > kWaitNs) return false;
+        if (global_ns() - t0 > lim) return false;
     return true;
+}
+
+__device__ __forceinline__ void mbar_inval(uint64_t *bar)
+{
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 // contiguous global -> shared copy; dst, src 16-byte aligned, bytes % 16 == 0

@@ -32,7 +32,8 @@ typedef enum imr_status {
     IMR_ERR_CUDA = 4,              /* a CUDA runtime call failed              */
     IMR_ERR_NOT_INITIALIZED = 5,   /* task queue used before imr_queue_init   */
     IMR_ERR_QUEUE = 6,             /* task queue / serving loop failure       */
-    IMR_ERR_DEVICE_TIMEOUT = 7     /* a bounded device-side wait gave up      */
+    IMR_ERR_DEVICE_TIMEOUT = 7,    /* a bounded device-side wait gave up      */
+    IMR_ERR_CANCELLED = 8          /* the request was cancelled (engine)      */
 } imr_status;
 
 /* Parameters of one reconstruction, same meaning as the reference's
@@ -119,7 +120,23 @@ int imr_plan_profile(imr_plan *plan, int iters, void *stream, float *ms_row_pass
  * array touched once (row: X, g_prev in; g_prev, X out; mask in = 33 B/px;
  * column: X, modulus in; X out = 20 B/px). */
 int imr_plan_pass_bytes(imr_plan *plan, double *row_bytes, double *col_bytes);
+/* Limit of every bounded device-side copy wait of the plan's passes, in
+ * nanoseconds (0 = the default, 0.5 s).  A wait that runs out records
+ * IMR_ERR_DEVICE_TIMEOUT in the plan's state (imr_plan_stats returns it);
+ * the pass waits, bounded by the default limit, for its copies still in
+ * flight and returns, so the context stays usable.  Takes effect for the
+ * next execution; synchronous.  The reference has no such bound: it exits
+ * the process on any CUDA error (src/imresh/libs/cudacommon.cu:39-56). */
+int imr_plan_set_wait_limit(imr_plan *plan, unsigned long long limit_ns);
 int imr_plan_destroy(imr_plan *plan);
+
+/* Self-check of the bounded wait the pipelined passes rely on: one thread
+ * waits, bounded by limit_ns (0 = 0.5 s), on a device barrier that nothing
+ * completes.  Returns IMR_ERR_DEVICE_TIMEOUT (the expected outcome) with the
+ * nanoseconds waited in *elapsed_ns, leaving the context usable; anything
+ * else means the bound does not work.  Synchronous.  No counterpart in the
+ * reference. */
+int imr_bounded_wait_check(unsigned long long limit_ns, unsigned long long *elapsed_ns, void *stream);
 
 /* ------------------------------------------------------------------------
  * Kernel-level entry points (device buffers, asynchronous on `stream`).
@@ -220,10 +237,14 @@ void imr_free_image(float *data);
  * For callers that cannot call cudaMalloc (memory owned by a fixed arena or a
  * framework allocator, loops that must not take the driver's allocation
  * locks, processes that reserve all device memory up front).  d_modulus and
- * d_out are DEVICE buffers of W*H floats owned by the caller; all other
- * working memory is a static device array of the library, so W*H is limited
- * to 512*512 pixels (IMR_ERR_UNSUPPORTED_SIZE beyond, with a message in
- * imr_last_error) and nCycles to 1024.  Asynchronous on `stream`.  The first
+ * d_out are DEVICE buffers of W*H floats owned by the caller; they may be the
+ * same buffer (the modulus is copied first, so the call can work in place
+ * like the reference's cudaShrinkWrap).  All other working memory is a static
+ * device array of the library (about 10 MB), so W*H is limited to 512*512
+ * pixels, nCycles to 1024, and W and H to lengths of the form 2^a 3^b 5^c 7^d
+ * (lengths with a larger prime factor need per-length tables that would have
+ * to be allocated): IMR_ERR_UNSUPPORTED_SIZE or IMR_ERR_INVALID_VALUE beyond,
+ * with a message in imr_last_error.  Asynchronous on `stream`.  The first
  * call on a device looks up the array's address and sets kernel attributes:
  * make it before any stream capture.  All calls share the one array: calls
  * whose GPU work overlaps (different streams, unordered host threads) race;
@@ -231,6 +252,14 @@ void imr_free_image(float *data);
  */
 int imr_shrink_wrap_noalloc(const float *d_modulus, float *d_out, unsigned W, unsigned H,
                             const imr_params *params, void *stream);
+/* Status of the last imr_shrink_wrap_noalloc call on the current device (it
+ * synchronises `stream`, which should be the call's stream): the cycles whose
+ * HIO block ran and was error-tested, the error after each of them (up to cap
+ * floats; errors may be NULL), and IMR_ERR_DEVICE_TIMEOUT when a bounded
+ * device-side copy wait gave up during that call (its output is then not a
+ * valid reconstruction).  Reads the library's static array only; allocates
+ * nothing. */
+int imr_shrink_wrap_noalloc_stats(void *stream, int *cycles_done, float *errors, int cap);
 
 /* ------------------------------------------------------------------------
  * Batched, continuously-admitting engine (the served form of the path).
@@ -238,9 +267,13 @@ int imr_shrink_wrap_noalloc(const float *d_modulus, float *d_out, unsigned W, un
  * (imresh::io::taskQueue*, src/imresh/io/taskQueue.cu:91-251) with device-
  * resident state for every admitted reconstruction: one imr_engine_step runs
  * one shrink-wrap cycle of every active reconstruction, whatever their sizes,
- * admits pending requests while the device-memory budget allows, and retires
- * finished ones (their Re(g') is copied to the caller's h_out).  Not thread
- * safe: drive one engine from one thread.
+ * as ONE CUDA graph launch (captured when the active set changes, replayed
+ * otherwise), admits pending requests while the device-memory budget allows,
+ * and retires finished ones (their Re(g') is copied to the caller's h_out).
+ * Finishing is decided on the device; the host reads every job's state
+ * asynchronously and acts on it two steps later, so a step returns without
+ * waiting for the GPU (at most two steps are queued).  Not thread safe: drive
+ * one engine from one thread.
  */
 typedef struct imr_engine imr_engine;
 
@@ -250,14 +283,26 @@ typedef struct imr_result {
     int cycles_done;       /* HIO blocks run and error-tested                */
     float last_error;      /* error after the last of them                   */
     double latency_ms;     /* submit -> result in h_out                      */
-    int status;            /* imr_status of this reconstruction              */
+    int status;            /* imr_status of this reconstruction: 0, or
+                              IMR_ERR_DEVICE_TIMEOUT (a device wait gave up),
+                              IMR_ERR_OUT_OF_MEMORY (never admitted: its
+                              memory was not available with nothing else
+                              running), IMR_ERR_CANCELLED                   */
 } imr_result;
 
 typedef struct imr_engine_info {
-    int pending, active, done;
+    int pending;           /* submitted, not admitted yet                    */
+    int active;            /* admitted, result not yet handed over           */
+    int done;              /* results waiting for imr_engine_poll            */
     size_t device_bytes_used, device_bytes_peak, device_bytes_budget;
-    long launches;         /* kernel launches issued so far                  */
+    long launches;         /* kernels run so far (a graph's count once per step) */
     long steps;
+    long host_launches;    /* launch calls the host made (a step graph counts once) */
+    long kernels_per_step; /* kernels in the current step graph              */
+    long graph_builds;     /* step graphs instantiated                       */
+    long graph_updates;    /* step graphs updated in place (same shape)      */
+    long alloc_failures;   /* admissions whose device allocation failed      */
+    int resident;          /* reconstructions holding device memory          */
 } imr_engine_info;
 
 /* device_bytes: admission budget (0 = 80 % of the free device memory);
@@ -267,14 +312,28 @@ int imr_engine_create(imr_engine **engine, size_t device_bytes, int max_jobs, vo
  * request is admitted, h_out (W*H floats) until its result is polled. */
 int imr_engine_submit(imr_engine *engine, const float *h_modulus, float *h_out, unsigned W,
                       unsigned H, const imr_params *params, long long tag);
-/* Admit, run one cycle of every active reconstruction, retire finished ones.
- * Synchronous. */
+/* Retire what had finished two steps ago, admit, launch one cycle of every
+ * active reconstruction.  Returns once the step is queued (it waits only for
+ * the step before the previous one). */
 int imr_engine_step(imr_engine *engine);
-/* Step until nothing is pending or active. */
+/* Step until nothing is pending, running or being copied out. */
 int imr_engine_run(imr_engine *engine);
 /* Finished reconstructions since the last poll (up to max_results). */
 int imr_engine_poll(imr_engine *engine, imr_result *results, int max_results, int *n_results);
 int imr_engine_stats(imr_engine *engine, imr_engine_info *info);
+/* Cancel a pending or running request between steps: it is reported by
+ * imr_engine_poll with status IMR_ERR_CANCELLED, its h_out is not written,
+ * its device memory is released after the steps already queued.  Returns
+ * IMR_ERR_INVALID_VALUE (with a message) when no pending or running request
+ * has this tag.  No counterpart in the reference (its tasks cannot be
+ * stopped). */
+int imr_engine_cancel(imr_engine *engine, long long tag);
+/* Host-side fault injection for tests of the failure paths: the device
+ * allocations of the next `count` admissions fail as if the device were out
+ * of memory.  A request whose allocation fails waits in the queue while
+ * other reconstructions run (their retirement frees memory) and is retried;
+ * with nothing else running it finishes with IMR_ERR_OUT_OF_MEMORY. */
+int imr_engine_inject_alloc_failures(imr_engine *engine, int count);
 /* Suspend / resume of one reconstruction (for preemption and restart).  Between
  * steps, a running reconstruction (`tag` of an active request) is saved into a
  * HOST buffer of imr_engine_snapshot_size bytes: its iterate, g_prev, modulus,
@@ -283,8 +342,10 @@ int imr_engine_stats(imr_engine *engine, imr_engine_info *info);
  * device memory (no result is reported for it).  resume queues the saved
  * reconstruction into this or another engine; it continues from the saved
  * cycle, bit-identical to an uninterrupted run, and its result goes to h_out
- * (W*H floats) under the saved tag.  Synchronous.  No counterpart in the
- * reference (its tasks cannot be interrupted). */
+ * (W*H floats) under the saved tag.  A reconstruction that has already
+ * finished on the device cannot be saved (IMR_ERR_INVALID_VALUE).
+ * Synchronous.  No counterpart in the reference (its tasks cannot be
+ * interrupted). */
 int imr_engine_snapshot_size(imr_engine *engine, long long tag, size_t *bytes);
 int imr_engine_checkpoint(imr_engine *engine, long long tag, void *h_buf, size_t capacity);
 int imr_engine_suspend(imr_engine *engine, long long tag, void *h_buf, size_t capacity);

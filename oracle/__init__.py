@@ -31,12 +31,17 @@ _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
 
 
+def reference_tree() -> str:
+    """The reference project's source tree: $IMRESH_REF, else the directory
+    ``reference`` beside this repository."""
+    return os.environ.get("IMRESH_REF") or os.path.normpath(os.path.join(_HERE, "..", "..", "reference"))
+
+
 def build(ref: bool = True) -> None:
     """Compile liboracle.so and, where the reference tree exists, _ref/."""
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
-    if ref and os.path.isdir(os.environ.get("IMRESH_REF", "/root/reference")):
-        subprocess.run(["make", "-s", "-C", _HERE, "ref",
-                        "REF=" + os.environ.get("IMRESH_REF", "/root/reference")], check=True)
+    if ref and os.path.isdir(reference_tree()):
+        subprocess.run(["make", "-s", "-C", _HERE, "ref", "REF=" + reference_tree()], check=True)
 
 
 class _HioTrace(C.Structure):

@@ -70,7 +70,7 @@ def test_admission_under_memory_budget(cuda):
         info = eng.info()
         if info["pending"] == 0 and info["active"] == 0:
             break
-        assert info["active"] <= 2
+        assert info["resident"] <= 2
         eng.step()
         steps += 1
     res = {r["tag"]: r for r in eng.poll()}
