@@ -89,6 +89,9 @@ def lib() -> C.CDLL:
     L.imr_plan_profile.argtypes = [vp, i, vp, C.POINTER(f), C.POINTER(f)]
     L.imr_plan_pass_bytes.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.imr_fft2d.argtypes = [vp, u, u, i, vp]
+    L.imr_fft2d_split.argtypes = [vp, u, u, i, i, vp]
+    L.imr_plan_set_precision.argtypes = [vp, i]
+    L.imr_plan_set_wait_limit.argtypes = [vp, C.c_ulonglong]
     L.imr_gaussian_blur.argtypes = [vp, vp, u, u, C.c_double, i, vp]
     L.imr_gaussian_weights.argtypes = [C.c_double, vp, i]
     L.imr_vector_max.argtypes = [vp, C.c_size_t, C.POINTER(f), vp]
@@ -201,6 +204,10 @@ class Plan:
                "imr_plan_stats")
         return n.value, errs[:n.value]
 
+    def set_precision(self, precision: int):
+        """Column-pass arithmetic: PREC_FP32 (default), PREC_BF16X3 or PREC_FP16X3."""
+        _check(lib().imr_plan_set_precision(self._h, precision), "imr_plan_set_precision")
+
     def launches(self) -> int:
         n = C.c_long()
         _check(lib().imr_plan_launches(self._h, C.byref(n)), "imr_plan_launches")
@@ -246,6 +253,15 @@ def fft2d(d_data, width: int, height: int, sign: int, stream=None):
     _check(lib().imr_fft2d(_ptr(d_data), width, height, sign, _stream(stream)), "imr_fft2d")
 
 
+PREC_FP32, PREC_BF16X3, PREC_FP16X3 = 0, 1, 2
+
+
+def fft2d_split(d_data, width: int, height: int, sign: int, precision: int = PREC_BF16X3, stream=None):
+    """fft2d with the column transform on the split-precision tensor-core passes."""
+    _check(lib().imr_fft2d_split(_ptr(d_data), width, height, sign, precision, _stream(stream)),
+           "imr_fft2d_split")
+
+
 def gaussian_blur(d_data, d_tmp, width: int, height: int, sigma: float, axes: int = 3, stream=None):
     _check(lib().imr_gaussian_blur(_ptr(d_data), _ptr(d_tmp), width, height, float(sigma), axes,
                                    _stream(stream)), "imr_gaussian_blur")
@@ -276,7 +292,8 @@ class CEngineInfo(C.Structure):
                 ("device_bytes_used", C.c_size_t), ("device_bytes_peak", C.c_size_t),
                 ("device_bytes_budget", C.c_size_t), ("launches", C.c_long), ("steps", C.c_long),
                 ("host_launches", C.c_long), ("kernels_per_step", C.c_long), ("graph_builds", C.c_long),
-                ("graph_updates", C.c_long), ("alloc_failures", C.c_long), ("resident", C.c_int)]
+                ("graph_updates", C.c_long), ("alloc_failures", C.c_long), ("resident", C.c_int),
+                ("resident_px", C.c_size_t), ("last_step_ms", C.c_double), ("ms_per_mpx", C.c_double)]
 
 
 def _engine_sigs(L):
@@ -295,6 +312,8 @@ def _engine_sigs(L):
     L.imr_engine_resume.argtypes = [vp, vp, C.c_size_t, vp]
     L.imr_engine_cancel.argtypes = [vp, C.c_longlong]
     L.imr_engine_inject_alloc_failures.argtypes = [vp, C.c_int]
+    L.imr_engine_set_admission.argtypes = [vp, C.c_size_t]
+    L.imr_engine_set_step_target.argtypes = [vp, C.c_double]
 
 
 class Engine:
@@ -375,6 +394,14 @@ class Engine:
     def cancel(self, tag: int):
         """Cancel a pending or running request (reported with IMR_ERR_CANCELLED)."""
         _check(lib().imr_engine_cancel(self._h, tag), "imr_engine_cancel")
+
+    def set_admission(self, max_active_pixels: int):
+        """Admit requests only while the resident pixels stay within the bound (0: none)."""
+        _check(lib().imr_engine_set_admission(self._h, max_active_pixels), "imr_engine_set_admission")
+
+    def set_step_target(self, ms: float):
+        """Admit requests only while the predicted step time stays within `ms` (0: off)."""
+        _check(lib().imr_engine_set_step_target(self._h, float(ms)), "imr_engine_set_step_target")
 
     def inject_alloc_failures(self, count: int):
         """Make the device allocations of the next `count` admissions fail (tests)."""

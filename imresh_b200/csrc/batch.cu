@@ -50,11 +50,12 @@ static double now_ms()
     return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
 }
 
-// Pinned host staging for one result (reused once its copy is complete).
+// Pinned host staging for the results retired together (one chunk per
+// retirement batch; reused once all its copies are complete).
 struct Staging {
     char *p = nullptr;
     size_t cap = 0;
-    bool busy = false;
+    int busy = 0;   // results in it not yet handed over
 };
 
 struct EJob {
@@ -73,7 +74,8 @@ struct EJob {
     int status = IMR_SUCCESS;
     long admit_step = -1;       // its state was set before this step's state copy: older copies are stale
     long copy_step = -1;        // retiring: its result copy precedes this step's status copy
-    int staging = -1;           // retiring: index of its pinned staging buffer (-1: direct copy)
+    int staging = -1;           // retiring: index of its pinned staging chunk (-1: direct copy)
+    size_t staging_off = 0;     // its place in that chunk
     std::vector<char> resume;   // snapshot to continue from (empty: a new request)
 };
 
@@ -157,6 +159,16 @@ struct imr_engine {
     int sms = 148;
     int inject_alloc_fail = 0;      // the next admissions whose allocation is made to fail
     long alloc_failures = 0;
+    size_t max_active_px = 0;       // bound on the pixels of the resident requests (0: none)
+    size_t active_px = 0;
+    // admission by measured step time: every step's graph is timed on the
+    // device; ms_per_px follows step ms / resident pixels (EWMA), and with a
+    // target step time the resident pixels are held to target / ms_per_px
+    double target_step_ms = 0.0;
+    double ms_per_px = 0.0;
+    cudaEvent_t ev_t0[2] = {nullptr, nullptr}, ev_t1[2] = {nullptr, nullptr};
+    size_t step_px[2] = {0, 0};
+    double last_step_ms = 0.0;
 };
 
 #define CKE(call)                      \
@@ -224,6 +236,11 @@ static int admit(imr_engine *E)
         EJob *j = E->pending.front();
         const bool idle = E->active.empty() && E->fresh.empty();
         if (E->used + j->S.bytes > E->budget && !idle) break;
+        const size_t px = (size_t)j->W * j->H;
+        if (E->max_active_px && E->active_px + px > E->max_active_px && !idle) break;
+        if (E->target_step_ms > 0 && E->ms_per_px > 0 &&
+            (double)(E->active_px + px) * E->ms_per_px > E->target_step_ms && !idle)
+            break;
         E->pending.pop_front();
         j->slot = E->free_slots.back();
         E->free_slots.pop_back();
@@ -252,6 +269,7 @@ static int admit(imr_engine *E)
         }
         E->used += j->S.bytes;
         E->peak = std::max(E->peak, E->used);
+        E->active_px += px;
         job_bind(j->J, j->S, j->arena, E->dst + j->slot);
         int rc = job_upload(j->J, j->S, j->arena, E->dj + j->slot, E->s);
         if (rc) return rc;
@@ -468,12 +486,13 @@ static int rebuild(imr_engine *E)
     return IMR_SUCCESS;
 }
 
-static int stage_index(imr_engine *E, size_t bytes)
+// A free pinned chunk of at least `bytes` (allocated when none is free).
+static int stage_chunk(imr_engine *E, size_t bytes)
 {
     for (size_t i = 0; i < E->staging.size(); ++i)
-        if (!E->staging[i].busy && E->staging[i].cap >= bytes) return (int)i;
+        if (E->staging[i].busy == 0 && E->staging[i].cap >= bytes) return (int)i;
     Staging st;
-    const size_t cap = std::max(bytes, (size_t)1 << 20);
+    const size_t cap = std::max(bytes, (size_t)16 << 20);
     if (cudaMallocHost(&st.p, cap) != cudaSuccess) {
         cudaGetLastError();
         return -2;
@@ -489,14 +508,24 @@ static int stage_index(imr_engine *E, size_t bytes)
 static int observe(imr_engine *E, const JobState *hs, long m)
 {
     E->synced_step = m;
+    if (hs && m >= 0) {   // the device time of step m (its events completed before its state copy)
+        const int q = (int)(m & 1);
+        float ms = 0.f;
+        if (E->step_px[q] && cudaEventElapsedTime(&ms, E->ev_t0[q], E->ev_t1[q]) == cudaSuccess) {
+            E->last_step_ms = ms;
+            const double r = ms / (double)E->step_px[q];
+            E->ms_per_px = E->ms_per_px > 0 ? 0.8 * E->ms_per_px + 0.2 * r : r;
+        }
+        cudaGetLastError();
+    }
     // result copies issued before step m's state copy are complete
     for (size_t i = 0; i < E->retiring.size();) {
         EJob *j = E->retiring[i];
         if (j->copy_step >= 0 && j->copy_step <= m) {
             const size_t b = (size_t)j->W * j->H * 4;
             if (j->staging >= 0) {
-                memcpy(j->h_out, E->staging[j->staging].p, b);
-                E->staging[j->staging].busy = false;
+                memcpy(j->h_out, E->staging[j->staging].p + j->staging_off, b);
+                --E->staging[j->staging].busy;
             }
             finish_now(E, j, j->status);
             E->retiring.erase(E->retiring.begin() + i);
@@ -505,7 +534,8 @@ static int observe(imr_engine *E, const JobState *hs, long m)
         }
     }
     if (!hs) return IMR_SUCCESS;
-    std::vector<EJob *> keep;
+    std::vector<EJob *> keep, out;
+    size_t staged_bytes = 0;
     for (EJob *j : E->active) {
         const JobState &st = hs[j->slot];
         if (m < j->admit_step || !(st.stop || st.err)) {
@@ -515,23 +545,37 @@ static int observe(imr_engine *E, const JobState *hs, long m)
         j->cycles_done = st.cycles_done;
         j->last_error = st.last_error;
         j->status = st.err ? IMR_ERR_DEVICE_TIMEOUT : IMR_SUCCESS;
-        const size_t b = (size_t)j->W * j->H * 4;
         cudaPointerAttributes pa;
         const bool pinned = cudaPointerGetAttributes(&pa, j->h_out) == cudaSuccess &&
                             (pa.type == cudaMemoryTypeHost || pa.type == cudaMemoryTypeManaged);
         cudaGetLastError();
-        j->staging = pinned ? -1 : stage_index(E, b);
-        if (j->staging == -2) {
-            set_error("engine result staging", cudaErrorMemoryAllocation);
-            return IMR_ERR_OUT_OF_MEMORY;
+        j->staging = pinned ? -1 : 0;
+        if (!pinned) {
+            j->staging_off = staged_bytes;
+            staged_bytes += ((size_t)j->W * j->H * 4 + 255) / 256 * 256;
         }
-        void *dst = j->staging >= 0 ? (void *)E->staging[j->staging].p : (void *)j->h_out;
-        if (j->staging >= 0) E->staging[j->staging].busy = true;
+        out.push_back(j);
+    }
+    if (out.empty()) return IMR_SUCCESS;
+    const int chunk = staged_bytes ? stage_chunk(E, staged_bytes) : -1;
+    if (chunk == -2) {
+        set_error("engine result staging", cudaErrorMemoryAllocation);
+        return IMR_ERR_OUT_OF_MEMORY;
+    }
+    for (EJob *j : out) {
+        const size_t b = (size_t)j->W * j->H * 4;
+        void *dst = j->h_out;
+        if (j->staging >= 0) {
+            j->staging = chunk;
+            ++E->staging[chunk].busy;
+            dst = E->staging[chunk].p + j->staging_off;
+        }
         CKE(cudaMemcpyAsync(dst, j->J.out, b, cudaMemcpyDeviceToHost, E->s));
         CKE(cudaFreeAsync(j->arena, E->s));
         j->arena = nullptr;
         j->copy_step = E->steps;   // the copy precedes the state copy of the next step launched
         E->used -= j->S.bytes;
+        E->active_px -= (size_t)j->W * j->H;
         E->free_slots.push_back(j->slot);
         E->retiring.push_back(j);
         E->dirty = true;
@@ -614,6 +658,8 @@ int imr_engine_create(imr_engine **out, size_t device_bytes, int max_jobs, void 
         e = cudaMallocHost(&E->hst[q], sizeof(JobState) * max_jobs);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&E->ev_st[q], cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&E->ev_lists[q], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreate(&E->ev_t0[q]);
+        if (e == cudaSuccess) e = cudaEventCreate(&E->ev_t1[q]);
     }
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&E->cs, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMemset(E->dst, 0, sizeof(JobState) * max_jobs);
@@ -675,10 +721,13 @@ int imr_engine_step(imr_engine *E)
     CKE(cudaGetLastError());
     E->init_groups.clear();
     E->fresh.clear();
+    const int q = (int)(n & 1);
+    CKE(cudaEventRecord(E->ev_t0[q], E->s));
     CKE(cudaGraphLaunch(E->gexec, E->s));
+    CKE(cudaEventRecord(E->ev_t1[q], E->s));
+    E->step_px[q] = E->active_px;
     ++E->host_launches;
     E->launches += E->kernels_per_step;
-    const int q = (int)(n & 1);
     CKE(cudaMemcpyAsync(E->hst[q], E->dst, sizeof(JobState) * E->max_slots, cudaMemcpyDeviceToHost, E->s));
     CKE(cudaEventRecord(E->ev_st[q], E->s));
     E->st_step[q] = n;
@@ -739,9 +788,24 @@ int imr_engine_cancel(imr_engine *E, long long tag)
     CKE(cudaFreeAsync(j->arena, E->s));
     j->arena = nullptr;
     E->used -= j->S.bytes;
+    E->active_px -= (size_t)j->W * j->H;
     E->free_slots.push_back(j->slot);
     E->dirty = true;
     finish_now(E, j, IMR_ERR_CANCELLED);
+    return IMR_SUCCESS;
+}
+
+int imr_engine_set_admission(imr_engine *E, size_t max_active_pixels)
+{
+    if (!E) return IMR_ERR_INVALID_VALUE;
+    E->max_active_px = max_active_pixels;
+    return IMR_SUCCESS;
+}
+
+int imr_engine_set_step_target(imr_engine *E, double target_step_ms)
+{
+    if (!E || target_step_ms < 0) return IMR_ERR_INVALID_VALUE;
+    E->target_step_ms = target_step_ms;
     return IMR_SUCCESS;
 }
 
@@ -805,6 +869,7 @@ int imr_engine_suspend(imr_engine *E, long long tag, void *h_buf, size_t cap)
     CKE(cudaFreeAsync(j->arena, E->s));
     CKE(cudaStreamSynchronize(E->s));
     E->used -= j->S.bytes;
+    E->active_px -= (size_t)j->W * j->H;
     E->free_slots.push_back(j->slot);
     E->dirty = true;
     delete j;
@@ -853,6 +918,9 @@ int imr_engine_stats(imr_engine *E, imr_engine_info *st)
     st->graph_updates = E->graph_updates;
     st->alloc_failures = E->alloc_failures;
     st->resident = (int)E->active.size();
+    st->resident_px = E->active_px;
+    st->last_step_ms = E->last_step_ms;
+    st->ms_per_mpx = E->ms_per_px * 1e6;
     return IMR_SUCCESS;
 }
 
@@ -878,6 +946,8 @@ int imr_engine_destroy(imr_engine *E)
         if (E->h_lists[q]) cudaFreeHost(E->h_lists[q]);
         if (E->ev_st[q]) cudaEventDestroy(E->ev_st[q]);
         if (E->ev_lists[q]) cudaEventDestroy(E->ev_lists[q]);
+        if (E->ev_t0[q]) cudaEventDestroy(E->ev_t0[q]);
+        if (E->ev_t1[q]) cudaEventDestroy(E->ev_t1[q]);
     }
     for (auto &st : E->staging)
         if (st.p) cudaFreeHost(st.p);

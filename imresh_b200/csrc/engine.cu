@@ -264,9 +264,18 @@ static ColKernels col_set()
 {
     if constexpr (N >= 128 && N <= 4096 && is_pow2(N)) {   // 16 values per thread in the pipelined pass
         constexpr int T = pcol16_nbt(N);
-        return ColKernels{k_col_r<N>, k_col_init_r<N>, k_fft_cols_r<-1, N>, k_fft_cols_r<+1, N>,
-                          rcol_nb(N), rcol_threads(N), rcol_smem(N), k_col_p16<N, T>, pcol16_smem<N, T>(),
-                          pcol_box_rows(N), 0, pcol16_threads(N, T), 0, T, 1};
+        ColKernels k{k_col_r<N>, k_col_init_r<N>, k_fft_cols_r<-1, N>, k_fft_cols_r<+1, N>,
+                     rcol_nb(N), rcol_threads(N), rcol_smem(N), k_col_p16<N, T>, pcol16_smem<N, T>(),
+                     pcol_box_rows(N), 0, pcol16_threads(N, T), 0, T, 1};
+        if constexpr (N >= 256) {   // split-precision tensor-core variants
+            k.p_col_tc[0] = k_col_tc<N, T, kPrecBf16x3, 0>;
+            k.p_col_tc[1] = k_col_tc<N, T, kPrecFp16x3, 0>;
+            k.fft_tc[0][0] = k_col_tc<N, T, kPrecBf16x3, 1>;
+            k.fft_tc[0][1] = k_col_tc<N, T, kPrecBf16x3, 2>;
+            k.fft_tc[1][0] = k_col_tc<N, T, kPrecFp16x3, 1>;
+            k.fft_tc[1][1] = k_col_tc<N, T, kPrecFp16x3, 2>;
+        }
+        return k;
     } else if constexpr (N >= 16 && is_pow2(N))
         return ColKernels{k_col_r<N>, k_col_init_r<N>, k_fft_cols_r<-1, N>, k_fft_cols_r<+1, N>,
                           rcol_nb(N), rcol_threads(N), rcol_smem(N), k_col_p<N>, pcol_smem<N>(),
@@ -467,6 +476,11 @@ int ensure_kernel_attributes()
         if (e == cudaSuccess && r.p_hio_fix) e = allow_smem(r.p_hio_fix);
         if (e == cudaSuccess && r.p_finish) e = allow_smem(r.p_finish);
         if (e == cudaSuccess && c.p_col) e = allow_smem(c.p_col);
+        for (int pr = 0; pr < 2; ++pr) {
+            if (e == cudaSuccess && c.p_col_tc[pr]) e = allow_smem(c.p_col_tc[pr]);
+            for (int d = 0; d < 2; ++d)
+                if (e == cudaSuccess && c.fft_tc[pr][d]) e = allow_smem(c.fft_tc[pr][d]);
+        }
     }
     if (e == cudaSuccess) e = allow_smem(k_hblur);
     if (e != cudaSuccess) {
@@ -563,7 +577,14 @@ struct imr_plan {
     bool p_rows = false, p_cols = false;   // pipelined passes in use
     int g_row_first = 0, g_row = 0, g_col = 0;
     WorkList *Lrow = nullptr, *Lcol = nullptr, *Lvb = nullptr;   // device
+    int prec = 0;   // column pass: 0 FP32, 1 BF16 hi+lo tensor cores, 2 FP16 hi+lo tensor cores
 };
+
+// The pipelined column pass of the plan's precision.
+static void (*plan_col_kernel(const imr_plan *P))(const JobDev *, const WorkList *)
+{
+    return P->prec ? P->ck.p_col_tc[P->prec - 1] : P->ck.p_col;
+}
 
 static int plan_launch_cycle(imr_plan *P, cudaStream_t s)
 {
@@ -583,7 +604,7 @@ static int plan_launch_cycle(imr_plan *P, cudaStream_t s)
             (i == 0 ? rk.hio_first : rk.hio)<<<J.n_row_tiles, rk.threads, P->smem_row, s>>>(P->dj, P->Lrow);
         }
         if (P->p_cols)
-            ck.p_col<<<P->g_col, ck.p_threads, ck.p_smem, s>>>(P->dj, P->Lcol);
+            plan_col_kernel(P)<<<P->g_col, ck.p_threads, ck.p_smem, s>>>(P->dj, P->Lcol);
         else
             ck.col<<<J.n_col_tiles, ck.threads, P->smem_col, s>>>(P->dj, P->Lcol);
     }
@@ -771,6 +792,46 @@ int imr_plan_destroy(imr_plan *P)
     return IMR_SUCCESS;
 }
 
+// Capture the cycles as graphs: up to kPlanGraphCycles cycles per graph, so a
+// reconstruction is one or a few graph launches (no host work between
+// cycles), plus one graph for the remainder.  Replaces earlier graphs.
+static int plan_capture(imr_plan *P)
+{
+    if (P->gexec) cudaGraphExecDestroy(P->gexec);
+    if (P->graph) cudaGraphDestroy(P->graph);
+    if (P->gexec_rem) cudaGraphExecDestroy(P->gexec_rem);
+    if (P->graph_rem) cudaGraphDestroy(P->graph_rem);
+    P->gexec = P->gexec_rem = nullptr;
+    P->graph = P->graph_rem = nullptr;
+    const JobDev &J = P->hj;
+    P->chunk = J.n_cycles < kPlanGraphCycles ? J.n_cycles : kPlanGraphCycles;
+    P->n_chunks = P->chunk ? J.n_cycles / P->chunk : 0;
+    const int rem = P->chunk ? J.n_cycles % P->chunk : 0;
+    int rc = IMR_SUCCESS;
+    cudaStream_t cs;
+    cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+    for (int g = 0; g < 2 && e == cudaSuccess && rc == IMR_SUCCESS; ++g) {
+        const int cycles = g == 0 ? P->chunk : rem;
+        if (cycles == 0) continue;
+        cudaGraph_t &gr = g == 0 ? P->graph : P->graph_rem;
+        cudaGraphExec_t &gx = g == 0 ? P->gexec : P->gexec_rem;
+        e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) break;
+        for (int c = 0; c < cycles && rc == IMR_SUCCESS; ++c) rc = plan_launch_cycle(P, cs);
+        cudaError_t e2 = cudaStreamEndCapture(cs, &gr);
+        if (rc == IMR_SUCCESS && e2 == cudaSuccess)
+            e = cudaGraphInstantiate(&gx, gr, 0);
+        else if (e2 != cudaSuccess)
+            e = e2;
+    }
+    cudaStreamDestroy(cs);
+    if (e != cudaSuccess) {
+        set_error("graph capture", e);
+        return rc ? rc : IMR_ERR_CUDA;
+    }
+    return rc;
+}
+
 int imr_plan_create(imr_plan **out, unsigned W, unsigned H, const imr_params *params)
 {
     if (!out || W == 0 || H == 0) return IMR_ERR_INVALID_VALUE;
@@ -828,33 +889,9 @@ int imr_plan_create(imr_plan **out, unsigned W, unsigned H, const imr_params *pa
         imr_plan_destroy(P);
         return IMR_ERR_CUDA;
     }
-    // capture the cycles as graphs: up to kPlanGraphCycles cycles per graph, so a
-    // reconstruction is one or a few graph launches (no host work between
-    // cycles), plus one graph for the remainder
-    P->chunk = J.n_cycles < kPlanGraphCycles ? J.n_cycles : kPlanGraphCycles;
-    P->n_chunks = P->chunk ? J.n_cycles / P->chunk : 0;
-    const int rem = P->chunk ? J.n_cycles % P->chunk : 0;
-    cudaStream_t cs;
-    e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
-    for (int g = 0; g < 2 && e == cudaSuccess && rc == IMR_SUCCESS; ++g) {
-        const int cycles = g == 0 ? P->chunk : rem;
-        if (cycles == 0) continue;
-        cudaGraph_t &gr = g == 0 ? P->graph : P->graph_rem;
-        cudaGraphExec_t &gx = g == 0 ? P->gexec : P->gexec_rem;
-        e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
-        if (e != cudaSuccess) break;
-        for (int c = 0; c < cycles && rc == IMR_SUCCESS; ++c) rc = plan_launch_cycle(P, cs);
-        cudaError_t e2 = cudaStreamEndCapture(cs, &gr);
-        if (rc == IMR_SUCCESS && e2 == cudaSuccess)
-            e = cudaGraphInstantiate(&gx, gr, 0);
-        else if (e2 != cudaSuccess)
-            e = e2;
-    }
-    cudaStreamDestroy(cs);
-    if (e != cudaSuccess || rc != IMR_SUCCESS) {
-        if (e != cudaSuccess) set_error("graph capture", e);
+    if ((rc = plan_capture(P))) {
         imr_plan_destroy(P);
-        return rc ? rc : IMR_ERR_CUDA;
+        return rc;
     }
     *out = P;
     return IMR_SUCCESS;
@@ -966,7 +1003,7 @@ static cudaError_t profile_replay(imr_plan *P, int iters, bool split, cudaStream
                 P->rk.hio<<<J.n_row_tiles, P->rk.threads, P->smem_row, cs>>>(P->dj, P->Lrow);
             if (split) cudaEventRecordWithFlags(ev[k++], cs, cudaEventRecordExternal);
             if (P->p_cols)
-                P->ck.p_col<<<P->g_col, P->ck.p_threads, P->ck.p_smem, cs>>>(P->dj, P->Lcol);
+                plan_col_kernel(P)<<<P->g_col, P->ck.p_threads, P->ck.p_smem, cs>>>(P->dj, P->Lcol);
             else
                 P->ck.col<<<J.n_col_tiles, P->ck.threads, P->smem_col, cs>>>(P->dj, P->Lcol);
             if (split || i == iters - 1) cudaEventRecordWithFlags(ev[k++], cs, cudaEventRecordExternal);
@@ -1032,6 +1069,78 @@ int imr_plan_set_wait_limit(imr_plan *P, unsigned long long limit_ns)
     P->hj.wait_ns = limit_ns;
     // the captured graphs read the job description from device memory: no re-capture
     CK(cudaMemcpy(P->dj, &P->hj, sizeof(JobDev), cudaMemcpyHostToDevice));
+    return IMR_SUCCESS;
+}
+
+int imr_plan_set_precision(imr_plan *P, int precision)
+{
+    if (!P || precision < IMR_PREC_FP32 || precision > IMR_PREC_FP16X3) return IMR_ERR_INVALID_VALUE;
+    if (precision != IMR_PREC_FP32 && !(P->p_cols && P->ck.p_col_tc[precision - 1])) {
+        snprintf(g_last_error, sizeof(g_last_error),
+                 "split-precision column pass: height %d is not a power of two in 256..4096 with a pipelined "
+                 "column pass", P->H);
+        return IMR_ERR_UNSUPPORTED_SIZE;
+    }
+    if (precision == P->prec) return IMR_SUCCESS;
+    P->prec = precision;
+    CK(cudaDeviceSynchronize());
+    return plan_capture(P);
+}
+
+int imr_fft2d_split(void *d_data, unsigned W, unsigned H, int sign, int precision, void *stream)
+{
+    if (!d_data || W == 0 || H == 0 || (sign != 1 && sign != -1) || precision < IMR_PREC_BF16X3 ||
+        precision > IMR_PREC_FP16X3)
+        return IMR_ERR_INVALID_VALUE;
+    int rc = ensure_kernel_attributes();
+    if (rc) return rc;
+    const ColKernels ck = col_kernels((int)H);
+    auto kcol = ck.fft_tc[precision - 1][sign < 0 ? 0 : 1];
+    if (!kcol || W % (unsigned)ck.p_nb != 0 || ((uintptr_t)d_data & 15)) {
+        snprintf(g_last_error, sizeof(g_last_error),
+                 "imr_fft2d_split: H must be a power of two in 256..4096 and W a multiple of %d", ck.p_nb);
+        return IMR_ERR_UNSUPPORTED_SIZE;
+    }
+    FftPlanDev pr, pc;
+    if ((rc = make_fft_plan((int)W, pr)) || (rc = make_fft_plan((int)H, pc))) return rc;
+    JobDev J;
+    memset(&J, 0, sizeof(J));
+    J.W = (int)W;
+    J.H = (int)H;
+    J.X = (float2 *)d_data;
+    J.pcol = pc;
+    J.cpc = ck.p_nb;
+    J.n_col_tiles = (int)W / ck.p_nb;
+    if (!encode_tensor_map(&J.tmX, d_data, J.W, J.H, 8, ck.p_nb, ck.p_box_rows)) return IMR_ERR_UNSUPPORTED_SIZE;
+    cudaStream_t s = (cudaStream_t)stream;
+    char *dev = nullptr;
+    const size_t jb = (sizeof(JobDev) + 255) / 256 * 256;
+    CK(cudaMallocAsync((void **)&dev, jb + 256 + 256, s));
+    JobDev *dj = (JobDev *)dev;
+    WorkList *dl = (WorkList *)(dev + jb);
+    JobState *dst = (JobState *)(dev + jb + 256);
+    J.st = dst;
+    const WorkList wl{nullptr, J.n_col_tiles};
+    CK(cudaMemcpyAsync(dj, &J, sizeof(JobDev), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(dl, &wl, sizeof(WorkList), cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(dst, 0, sizeof(JobState), s));
+    const int grid = persistent_grid((const void *)kcol, ck.p_threads, ck.p_smem, J.n_col_tiles);
+    if (sign < 0) {
+        if ((rc = fft_passes((float2 *)d_data, (int)W, (int)H, -1, 1, pr, pc, s))) return rc;
+        kcol<<<grid, ck.p_threads, ck.p_smem, s>>>(dj, dl);
+    } else {
+        kcol<<<grid, ck.p_threads, ck.p_smem, s>>>(dj, dl);
+        if ((rc = fft_passes((float2 *)d_data, (int)W, (int)H, +1, 1, pr, pc, s))) return rc;
+    }
+    CK(cudaGetLastError());
+    JobState st;
+    CK(cudaMemcpyAsync(&st, dst, sizeof(JobState), cudaMemcpyDeviceToHost, s));
+    CK(cudaFreeAsync(dev, s));
+    CK(cudaStreamSynchronize(s));
+    if (st.err) {
+        snprintf(g_last_error, sizeof(g_last_error), "imr_fft2d_split: a device-side copy wait timed out");
+        return IMR_ERR_DEVICE_TIMEOUT;
+    }
     return IMR_SUCCESS;
 }
 

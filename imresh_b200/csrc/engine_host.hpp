@@ -61,6 +61,11 @@ struct ColKernels {
     int bs_m;        // Bluestein work length (0: direct transform)
     int p_nb;        // columns per tile of the pipelined pass (its TMA box width)
     int p_mt;        // 1: the pipelined pass reads the modulus from JobDev::Mt when set
+    // split-precision tensor-core column passes ([0] BF16 hi+lo, [1] FP16 hi+lo;
+    // same launch shape as p_col) and their stand-alone forward / inverse
+    // column transforms; null where the length has none
+    void (*p_col_tc[2])(const JobDev *, const WorkList *);
+    void (*fft_tc[2][2])(const JobDev *, const WorkList *);   // [precision][0 forward, 1 inverse]
 };
 RowKernels row_kernels(int N);
 ColKernels col_kernels(int N);

@@ -2236,3 +2236,5 @@ k_col_p16(const JobDev *jobs, const WorkList *L)
 }
 
 }  // namespace imr
+
+#include "kernels_tc.cuh"

@@ -128,6 +128,24 @@ int imr_plan_pass_bytes(imr_plan *plan, double *row_bytes, double *col_bytes);
  * next execution; synchronous.  The reference has no such bound: it exits
  * the process on any CUDA error (src/imresh/libs/cudacommon.cu:39-56). */
 int imr_plan_set_wait_limit(imr_plan *plan, unsigned long long limit_ns);
+/* Arithmetic of the plan's column pass (forward column FFT, modulus
+ * projection, inverse column FFT -- the cuFFT pair around the modulus step,
+ * src/imresh/algorithms/cuda/cudaShrinkWrap.cu:319,343):
+ *   IMR_PREC_FP32     FP32 FFT on the CUDA cores (the default; the drop-in);
+ *   IMR_PREC_BF16X3   radix-16 stages as DFT-16 matrix products on the tensor
+ *                     cores, inputs and DFT matrix split into BF16 hi + lo,
+ *                     three products accumulated in FP32;
+ *   IMR_PREC_FP16X3   the same in FP16 hi + lo with a power-of-two scale per
+ *                     tile and stage.
+ * Twiddles, the last stage of radix < 16, the modulus step and every error
+ * sum stay FP32 / FP64.  The split-precision passes need a height that is a
+ * power of two in 256..4096 with the pipelined column pass
+ * (IMR_ERR_UNSUPPORTED_SIZE otherwise).  Re-captures the plan's graphs;
+ * synchronous. */
+#define IMR_PREC_FP32 0
+#define IMR_PREC_BF16X3 1
+#define IMR_PREC_FP16X3 2
+int imr_plan_set_precision(imr_plan *plan, int precision);
 int imr_plan_destroy(imr_plan *plan);
 
 /* Self-check of the bounded wait the pipelined passes rely on: one thread
@@ -144,6 +162,12 @@ int imr_bounded_wait_check(unsigned long long limit_ns, unsigned long long *elap
 /* Unnormalised 2D C2C transform in place; sign -1 forward, +1 inverse
  * (cufftExecC2C FORWARD / INVERSE as used at cudaShrinkWrap.cu:232,319,343). */
 int imr_fft2d(void *d_data, unsigned W, unsigned H, int sign, void *stream);
+/* The same 2D transform with the column transform on the split-precision
+ * tensor-core passes (precision IMR_PREC_BF16X3 or IMR_PREC_FP16X3; rows
+ * stay FP32).  H: a power of two in 256..4096; W: a multiple of the column
+ * tile width (16 up to H = 512, 8 at 1024, 4 at 2048, 2 at 4096); d_data 16-byte
+ * aligned.  Synchronous. */
+int imr_fft2d_split(void *d_data, unsigned W, unsigned H, int sign, int precision, void *stream);
 /* Separable Gaussian blur in place, clamp border, rows then columns
  * (cudaGaussianBlur, src/imresh/algorithms/cuda/cudaGaussian.cu:1044-1057);
  * axes: 1 rows only, 2 columns only, 3 both.  d_tmp: W*H floats of scratch. */
@@ -303,6 +327,9 @@ typedef struct imr_engine_info {
     long graph_updates;    /* step graphs updated in place (same shape)      */
     long alloc_failures;   /* admissions whose device allocation failed      */
     int resident;          /* reconstructions holding device memory          */
+    size_t resident_px;    /* their pixels                                   */
+    double last_step_ms;   /* device time of the last step whose state was read */
+    double ms_per_mpx;     /* step time per million resident pixels (running) */
 } imr_engine_info;
 
 /* device_bytes: admission budget (0 = 80 % of the free device memory);
@@ -328,6 +355,21 @@ int imr_engine_stats(imr_engine *engine, imr_engine_info *info);
  * has this tag.  No counterpart in the reference (its tasks cannot be
  * stopped). */
 int imr_engine_cancel(imr_engine *engine, long long tag);
+/* Bound on the work admitted at once: a pending request is admitted only
+ * while the pixels (W*H) of all resident requests, its own included, stay
+ * within max_active_pixels (0 = no bound: device memory alone decides), or
+ * when nothing else is running.  Each step advances every resident request
+ * by one cycle, so the step time -- and with it the latency of every admitted
+ * request -- grows with the admitted pixels; the bound caps it, and the
+ * requests beyond it wait in arrival order. */
+int imr_engine_set_admission(imr_engine *engine, size_t max_active_pixels);
+/* The same bound derived from the measured step time: every step's graph is
+ * timed on the device, the engine keeps a running cost per resident pixel,
+ * and admits a request only while the predicted step time stays within
+ * target_step_ms (0 = off) or nothing else is running.  A request's latency
+ * is then about its cycle count times the target, plus its wait in the
+ * queue. */
+int imr_engine_set_step_target(imr_engine *engine, double target_step_ms);
 /* Host-side fault injection for tests of the failure paths: the device
  * allocations of the next `count` admissions fail as if the device were out
  * of memory.  A request whose allocation fails waits in the queue while
