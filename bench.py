@@ -287,7 +287,7 @@ def run_plain_256(args, flush, stream):
     return r, {"M": M, "obj": obj, "out": out, "errors": errs}
 
 
-def run_batched(n_jobs: int = 512, plain_sample: int = 64):
+def run_batched(n_jobs: int = 512, plain_sample: int = 64, schedule: int = 0):
     """The uneven batch: n_jobs reconstructions, W and H each from
     {128,192,256,384,512}, 20-200 blobs, Poisson 1e7-1e9 photons, seed 2,
     64 cycles x 20 HIO.  Served by the batched engine (all jobs submitted at
@@ -311,6 +311,7 @@ def run_batched(n_jobs: int = 512, plain_sample: int = 64):
     eng.poll(len(first))
     eng.close()
     eng = imr.Engine()
+    eng.set_schedule(schedule)
     t0 = time.perf_counter()
     for i, M in enumerate(inputs):
         eng.submit(M, prm, tag=i)
@@ -417,7 +418,8 @@ def run_large_4096(args, flush, stream):
     return res, {"M": M, "obj": obj, "out1": keep}
 
 
-def run_served(n_req: int, rate_hz: float, seed: int = 4, max_side: int = 2048, max_active_px: int = 0):
+def run_served(n_req: int, rate_hz: float, seed: int = 4, max_side: int = 2048, max_active_px: int = 0,
+               schedule: int = 0, step_target_ms: float = 0.0):
     """Serving stream: n_req requests with Poisson arrivals at rate_hz;
     W, H log-uniform integers in [64, max_side] (any length: mixed radix or
     Bluestein), 0.5-3 blobs per 1000 px^2, Poisson 1e6-1e9 photons; each
@@ -435,8 +437,11 @@ def run_served(n_req: int, rate_hz: float, seed: int = 4, max_side: int = 2048, 
     arrivals = np.cumsum(rng.exponential(1.0 / rate_hz, n_req))
     prm = imr.Params(128, 1e-5, 0.9, 0.04, 0.2, 3.0, 0.01, 20)
     eng = imr.Engine()
+    eng.set_schedule(schedule)
     if max_active_px:
         eng.set_admission(max_active_px)
+    if step_target_ms:
+        eng.set_step_target(step_target_ms)
     done, nxt, lat, t0 = 0, 0, [], time.perf_counter()
     submit_t = {}
     peak_active, cycles = 0, []
@@ -465,7 +470,8 @@ def run_served(n_req: int, rate_hz: float, seed: int = 4, max_side: int = 2048, 
             "recon_per_s": n_req / wall, "latency_p50_ms": p50, "latency_p99_ms": p99,
             "latency_max_ms": float(np.max(lat)), "offered_rate_hz": rate_hz,
             "peak_resident": peak_active, "device_bytes_peak": info["device_bytes_peak"],
-            "max_active_px": max_active_px or None,
+            "max_active_px": max_active_px or None, "step_target_ms": step_target_ms or None,
+            "schedule": "chained" if schedule else "grouped",
             "mean_cycles": float(np.mean(cycles)), "steps": info["steps"], "kernels": info["launches"],
             "host_launches": info["host_launches"], "graph_builds": info["graph_builds"],
             "graph_updates": info["graph_updates"]}

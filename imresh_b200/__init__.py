@@ -254,6 +254,7 @@ def fft2d(d_data, width: int, height: int, sign: int, stream=None):
 
 
 PREC_FP32, PREC_BF16X3, PREC_FP16X3 = 0, 1, 2
+SCHEDULE_GROUPED, SCHEDULE_CHAINED = 0, 1
 
 
 def fft2d_split(d_data, width: int, height: int, sign: int, precision: int = PREC_BF16X3, stream=None):
@@ -314,6 +315,7 @@ def _engine_sigs(L):
     L.imr_engine_inject_alloc_failures.argtypes = [vp, C.c_int]
     L.imr_engine_set_admission.argtypes = [vp, C.c_size_t]
     L.imr_engine_set_step_target.argtypes = [vp, C.c_double]
+    L.imr_engine_set_schedule.argtypes = [vp, C.c_int]
 
 
 class Engine:
@@ -398,6 +400,10 @@ class Engine:
     def set_admission(self, max_active_pixels: int):
         """Admit requests only while the resident pixels stay within the bound (0: none)."""
         _check(lib().imr_engine_set_admission(self._h, max_active_pixels), "imr_engine_set_admission")
+
+    def set_schedule(self, schedule: int):
+        """SCHEDULE_GROUPED (default) or SCHEDULE_CHAINED step graphs."""
+        _check(lib().imr_engine_set_schedule(self._h, schedule), "imr_engine_set_schedule")
 
     def set_step_target(self, ms: float):
         """Admit requests only while the predicted step time stays within `ms` (0: off)."""

@@ -34,6 +34,7 @@
 #include <chrono>
 #include <deque>
 #include <map>
+#include <tuple>
 #include <vector>
 
 #include <stdio.h>
@@ -112,6 +113,17 @@ struct Group {
     int list_base = 0;             // index of this group's first WorkList header
 };
 
+// The jobs of one (row kernel, column kernel) class: their whole cycle --
+// finish, vertical blur, every row and column pass -- depends on nothing
+// outside the class, so in the chained schedule each class is one branch of
+// the step graph and the classes run concurrently.
+struct Chain {
+    Group row, col;
+    std::vector<WorkItem> vb;
+    int vb_base = 0;
+};
+constexpr int kBranchStreams = 16;
+
 }  // namespace imr
 
 using namespace imr;
@@ -157,6 +169,9 @@ struct imr_engine {
     long graph_builds = 0, graph_updates = 0;
     long steps = 0;
     int sms = 148;
+    int schedule = 0;                 // IMR_SCHEDULE_GROUPED / IMR_SCHEDULE_CHAINED
+    cudaStream_t bs[kBranchStreams] = {};
+    cudaEvent_t ev_fork = nullptr, ev_join[kBranchStreams] = {};
     int inject_alloc_fail = 0;      // the next admissions whose allocation is made to fail
     long alloc_failures = 0;
     size_t max_active_px = 0;       // bound on the pixels of the resident requests (0: none)
@@ -407,24 +422,67 @@ static int launch_cycle(imr_engine *E, cudaStream_t s, const WorkList *L, std::v
     return IMR_SUCCESS;
 }
 
+static void build_chains(const std::vector<EJob *> &jobs, std::vector<Chain> &out)
+{
+    std::map<std::tuple<const void *, int, const void *, int>, std::vector<EJob *>> by;
+    for (EJob *j : jobs) {
+        const void *ck = j->S.p_cols ? (const void *)j->S.ck.p_col : (const void *)j->S.ck.col;
+        by[std::make_tuple((const void *)j->S.rk.hio, j->S.p_rows ? 1 : 0, ck, j->S.p_cols ? 1 : 0)].push_back(j);
+    }
+    out.clear();
+    for (auto &kv : by) {
+        Chain c;
+        std::vector<Group> g;
+        build_groups(kv.second, true, g);
+        c.row = std::move(g[0]);
+        build_groups(kv.second, false, g);
+        c.col = std::move(g[0]);
+        for (EJob *j : kv.second)
+            for (int t = 0; t < j->J.n_vb_tiles; ++t) c.vb.push_back(WorkItem{j->slot, t});
+        out.push_back(std::move(c));
+    }
+}
+
+// One cycle of the jobs of one chain, on stream s.
+static int launch_chain(imr_engine *E, cudaStream_t s, const WorkList *L, Chain &c, long *kernels)
+{
+    std::vector<Group> rg(1), cg(1);
+    rg[0] = c.row;
+    cg[0] = c.col;
+    long k = 0;
+    const int rc = launch_cycle(E, s, L, rg, cg, c.vb_base, c.vb.size(), &k);
+    *kernels += k;
+    return rc;
+}
+
 // Rebuild the work lists of the active set and the newly admitted jobs'
 // column init, upload them (stream-ordered after the queued steps, which
 // still read the previous lists), and re-capture the step graph.
 static int rebuild(imr_engine *E)
 {
     std::vector<Group> rowg, colg;
-    build_groups(E->fresh, false, E->init_groups);
-    build_groups(E->active, true, rowg);
-    build_groups(E->active, false, colg);
+    std::vector<Chain> chains;
     std::vector<WorkItem> vb;
-    for (EJob *j : E->active)
-        for (int t = 0; t < j->J.n_vb_tiles; ++t) vb.push_back(WorkItem{j->slot, t});
+    build_groups(E->fresh, false, E->init_groups);
+    const bool chained = E->schedule == IMR_SCHEDULE_CHAINED;
+    if (chained) {
+        build_chains(E->active, chains);
+    } else {
+        build_groups(E->active, true, rowg);
+        build_groups(E->active, false, colg);
+        for (EJob *j : E->active)
+            for (int t = 0; t < j->J.n_vb_tiles; ++t) vb.push_back(WorkItem{j->slot, t});
+    }
     size_t n_items = vb.size(), n_lists = 1;
     for (auto *G : {&E->init_groups, &rowg, &colg})
         for (auto &g : *G) {
             n_items += g.items.size();
             n_lists += 1 + g.hio_count.size();
         }
+    for (auto &c : chains) {
+        n_items += c.vb.size() + c.row.items.size() + c.col.items.size();
+        n_lists += 3 + c.row.hio_count.size() + c.col.hio_count.size();
+    }
     int rc = grow(E, n_items, n_lists);
     if (rc) return rc;
     const int q = E->lists_parity;
@@ -443,6 +501,11 @@ static int rebuild(imr_engine *E)
     put(vb, {}, vb_base);
     for (auto *G : {&E->init_groups, &rowg, &colg})
         for (auto &g : *G) put(g.items, g.hio_count, g.list_base);
+    for (auto &c : chains) {
+        put(c.vb, {}, c.vb_base);
+        put(c.row.items, c.row.hio_count, c.row.list_base);
+        put(c.col.items, c.col.hio_count, c.col.list_base);
+    }
     if (ip) CKE(cudaMemcpyAsync(E->d_items, hi, ip * sizeof(WorkItem), cudaMemcpyHostToDevice, E->s));
     CKE(cudaMemcpyAsync(E->d_lists, hl, lp * sizeof(WorkList), cudaMemcpyHostToDevice, E->s));
     CKE(cudaEventRecord(E->ev_lists[q], E->s));
@@ -452,7 +515,24 @@ static int rebuild(imr_engine *E)
     cudaGraph_t g = nullptr;
     long kernels = 0;
     CKE(cudaStreamBeginCapture(E->cs, cudaStreamCaptureModeThreadLocal));
-    rc = launch_cycle(E, E->cs, E->d_lists, rowg, colg, vb_base, vb.size(), &kernels);
+    if (!chained) {
+        rc = launch_cycle(E, E->cs, E->d_lists, rowg, colg, vb_base, vb.size(), &kernels);
+    } else {
+        // one branch per chain (chains beyond the branch streams share them in turn)
+        cudaError_t e = cudaEventRecord(E->ev_fork, E->cs);
+        const int nb = std::min((int)chains.size(), kBranchStreams);
+        for (int b = 0; b < nb && e == cudaSuccess; ++b) e = cudaStreamWaitEvent(E->bs[b], E->ev_fork, 0);
+        for (size_t c = 0; c < chains.size() && e == cudaSuccess && rc == IMR_SUCCESS; ++c)
+            rc = launch_chain(E, E->bs[c % kBranchStreams], E->d_lists, chains[c], &kernels);
+        for (int b = 0; b < nb && e == cudaSuccess; ++b) {
+            e = cudaEventRecord(E->ev_join[b], E->bs[b]);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(E->cs, E->ev_join[b], 0);
+        }
+        if (e != cudaSuccess && rc == IMR_SUCCESS) {
+            set_error("engine step graph branches", e);
+            rc = IMR_ERR_CUDA;
+        }
+    }
     const cudaError_t ec = cudaStreamEndCapture(E->cs, &g);
     if (rc) {
         if (g) cudaGraphDestroy(g);
@@ -662,6 +742,11 @@ int imr_engine_create(imr_engine **out, size_t device_bytes, int max_jobs, void 
         if (e == cudaSuccess) e = cudaEventCreate(&E->ev_t1[q]);
     }
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&E->cs, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&E->ev_fork, cudaEventDisableTiming);
+    for (int b = 0; b < kBranchStreams && e == cudaSuccess; ++b) {
+        e = cudaStreamCreateWithFlags(&E->bs[b], cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&E->ev_join[b], cudaEventDisableTiming);
+    }
     if (e == cudaSuccess) e = cudaMemset(E->dst, 0, sizeof(JobState) * max_jobs);
     if (e != cudaSuccess) {
         set_error("engine create", e);
@@ -799,6 +884,16 @@ int imr_engine_set_admission(imr_engine *E, size_t max_active_pixels)
 {
     if (!E) return IMR_ERR_INVALID_VALUE;
     E->max_active_px = max_active_pixels;
+    return IMR_SUCCESS;
+}
+
+int imr_engine_set_schedule(imr_engine *E, int schedule)
+{
+    if (!E || (schedule != IMR_SCHEDULE_GROUPED && schedule != IMR_SCHEDULE_CHAINED)) return IMR_ERR_INVALID_VALUE;
+    if (schedule != E->schedule) {
+        E->schedule = schedule;
+        E->dirty = true;
+    }
     return IMR_SUCCESS;
 }
 
@@ -954,6 +1049,11 @@ int imr_engine_destroy(imr_engine *E)
     if (E->d_items) cudaFree(E->d_items);
     if (E->d_lists) cudaFree(E->d_lists);
     if (E->cs) cudaStreamDestroy(E->cs);
+    if (E->ev_fork) cudaEventDestroy(E->ev_fork);
+    for (int b = 0; b < kBranchStreams; ++b) {
+        if (E->bs[b]) cudaStreamDestroy(E->bs[b]);
+        if (E->ev_join[b]) cudaEventDestroy(E->ev_join[b]);
+    }
     if (E->pool) cudaMemPoolDestroy(E->pool);
     delete E;
     return IMR_SUCCESS;

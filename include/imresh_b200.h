@@ -355,6 +355,18 @@ int imr_engine_stats(imr_engine *engine, imr_engine_info *info);
  * has this tag.  No counterpart in the reference (its tasks cannot be
  * stopped). */
 int imr_engine_cancel(imr_engine *engine, long long tag);
+/* How a step's kernels are ordered in its graph.
+ * IMR_SCHEDULE_GROUPED (default): one launch per pass and image-side class
+ *   over all jobs of that class; the passes of one HIO iteration follow each
+ *   other for all jobs (fewest kernels per step).
+ * IMR_SCHEDULE_CHAINED: the jobs of each (row kernel, column kernel) class
+ *   form an independent branch of the graph running its whole cycle, so the
+ *   classes run concurrently and fill each other's pass tails (more kernels,
+ *   no step-wide order between classes).  Results are bit-identical either
+ *   way.  Takes effect at the next step. */
+#define IMR_SCHEDULE_GROUPED 0
+#define IMR_SCHEDULE_CHAINED 1
+int imr_engine_set_schedule(imr_engine *engine, int schedule);
 /* Bound on the work admitted at once: a pending request is admitted only
  * while the pixels (W*H) of all resident requests, its own included, stay
  * within max_active_pixels (0 = no bound: device memory alone decides), or

@@ -42,6 +42,14 @@ def build(ref: bool = True) -> None:
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
     if ref and os.path.isdir(reference_tree()):
         subprocess.run(["make", "-s", "-C", _HERE, "ref", "REF=" + reference_tree()], check=True)
+        subprocess.run(["make", "-s", "-C", _HERE, "examples", "REF=" + reference_tree()], check=True)
+
+
+def example(name: str):
+    """Path of the reference's example program `name` built by `make examples`
+    (oracle/_ref/examples), or None."""
+    path = os.path.join(_HERE, "_ref", "examples", name)
+    return path if os.path.exists(path) else None
 
 
 class _HioTrace(C.Structure):

@@ -67,12 +67,15 @@ def test_split_path_one_iteration_matches_oracle(cuda, prec, shape):
 
 @pytest.mark.parametrize("prec", PRECS)
 def test_split_path_error_curve_follows_fp32(cuda, prec):
-    """4 cycles x 20 iterations of the 2048^2 Poisson workload: the per-cycle
-    errors of cycles 0 and 1 within 1 % of the FP32 path's (before the runs
-    separate: the reference's own FP32 and FP64 runs agree to 0.1 % there),
-    those of cycles 2 and 3 within 7 % (separated runs: 12 reference runs
-    on inputs one ulp apart spread over 3.5 % at these cycles, and this
-    compares two members of that spread)."""
+    """4 cycles x 20 iterations of the 2048^2 Poisson workload: the error of
+    cycle 0 within 1 % of the FP32 path's [measured: 0.03 %], those of
+    cycles 1-3 within 7 %.  The split path's transforms are 1e-5 (BF16) and
+    3e-7 (FP16) from FP64 against the FP32 path's 2e-7, so its run leaves the
+    FP32 trajectory about a cycle earlier than FP32 runs leave each other
+    (measured at cycle 1: BF16 -2.7 %, FP16 -1.4 %, while 12 FP32 reference
+    runs on inputs one ulp apart agree within 0.2 % there); once separated,
+    runs differ by the ensemble spread (3.5 % over those 12 runs at cycles
+    2-3), and this compares two members of it."""
     M, _ = data.make_modulus(data.cfg1_spec(), 1)
     prm = imr.Params(4, FLT_MIN, 0.9, 0.04, 0.2, 3.0, 0.01, 20)
     a = imr.Plan(2048, 2048, prm)
@@ -83,8 +86,8 @@ def test_split_path_error_curve_follows_fp32(cuda, prec):
     _, es = a.stats()
     a.close()
     assert np.all(np.isfinite(out))
-    np.testing.assert_allclose(es[:2], e32[:2], rtol=0.01)
-    np.testing.assert_allclose(es[2:], e32[2:], rtol=0.07)
+    np.testing.assert_allclose(es[:1], e32[:1], rtol=0.01)
+    np.testing.assert_allclose(es[1:], e32[1:], rtol=0.07)
 
 
 def test_split_precision_rejects_unsupported_heights(cuda):
