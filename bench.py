@@ -287,7 +287,7 @@ def run_plain_256(args, flush, stream):
     return r, {"M": M, "obj": obj, "out": out, "errors": errs}
 
 
-def run_batched(n_jobs: int = 512, plain_sample: int = 64, schedule: int = 0):
+def run_batched(n_jobs: int = 512, plain_sample: int = 64, schedule: int = 0, tune_cache: str | None = None):
     """The uneven batch: n_jobs reconstructions, W and H each from
     {128,192,256,384,512}, 20-200 blobs, Poisson 1e7-1e9 photons, seed 2,
     64 cycles x 20 HIO.  Served by the batched engine (all jobs submitted at
@@ -312,6 +312,8 @@ def run_batched(n_jobs: int = 512, plain_sample: int = 64, schedule: int = 0):
     eng.close()
     eng = imr.Engine()
     eng.set_schedule(schedule)
+    if tune_cache is not None:
+        eng.set_autotune(True, tune_cache)
     t0 = time.perf_counter()
     for i, M in enumerate(inputs):
         eng.submit(M, prm, tag=i)
@@ -355,6 +357,10 @@ def run_batched(n_jobs: int = 512, plain_sample: int = 64, schedule: int = 0):
         "engine_host_launches_per_step": info["host_launches"] / max(info["steps"], 1),
         "engine_kernels_per_step": info["kernels_per_step"],
         "engine_graph_builds": info["graph_builds"] + info["graph_updates"],
+        "engine_device_seconds": info["device_ms"] / 1e3,
+        "engine_schedule": "chained" if info["schedule"] else "grouped", "engine_grid_pct": info["grid_pct"],
+        "engine_tuner": {"explored_steps": info["tune_explored"], "cache_hits": info["tune_cache_hits"]}
+                        if tune_cache is not None else None,
         "plain_recon_per_s": plain_sample / dt_plain, "plain_sample_jobs": plain_sample,
         "plain_latency_p50_ms": _lat_stats(lat)[0],
         "speedup_engine_vs_plain": (n_jobs / dt) / (plain_sample / dt_plain),
@@ -723,6 +729,8 @@ def main():
                     help="only run the serving stream with N requests and print its JSON")
     ap.add_argument("--ncu-case", type=int, default=0, metavar="N",
                     help="run one NxN reconstruction (1 cycle x 3 HIO) and exit: a small case for ncu")
+    ap.add_argument("--ncu-prec", type=int, default=0,
+                    help="column-pass precision of the ncu case (0 FP32, 1 BF16 hi+lo, 2 FP16 hi+lo)")
     args = ap.parse_args()
     if args.ncu_case:
         import torch
@@ -731,11 +739,12 @@ def main():
         n = args.ncu_case
         M, _ = data.make_modulus(data.BlobSpec(n, n, 60, 0.15 * n, (2.0, 2.0), (0.5, 1.0), None), 0)
         plan = imr.Plan(n, n, imr.Params(1, imr.FLT_MIN, 0.9, 0.04, 0.2, 3.0, 0.01, 3))
+        plan.set_precision(args.ncu_prec)
         d_m = torch.from_numpy(M).cuda()
         d_o = torch.empty_like(d_m)
         plan.execute(d_m, d_o)
         torch.cuda.synchronize()
-        print(json.dumps({"ncu_case": n, "checksum": float(d_o.abs().sum())}))
+        print(json.dumps({"ncu_case": n, "precision": args.ncu_prec, "checksum": float(d_o.abs().sum())}))
         return
     if args.serve:
         import torch

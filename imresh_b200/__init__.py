@@ -294,7 +294,9 @@ class CEngineInfo(C.Structure):
                 ("device_bytes_budget", C.c_size_t), ("launches", C.c_long), ("steps", C.c_long),
                 ("host_launches", C.c_long), ("kernels_per_step", C.c_long), ("graph_builds", C.c_long),
                 ("graph_updates", C.c_long), ("alloc_failures", C.c_long), ("resident", C.c_int),
-                ("resident_px", C.c_size_t), ("last_step_ms", C.c_double), ("ms_per_mpx", C.c_double)]
+                ("resident_px", C.c_size_t), ("last_step_ms", C.c_double), ("ms_per_mpx", C.c_double),
+                ("device_ms", C.c_double), ("schedule", C.c_int), ("grid_pct", C.c_int),
+                ("tune_explored", C.c_long), ("tune_cache_hits", C.c_long)]
 
 
 def _engine_sigs(L):
@@ -316,6 +318,7 @@ def _engine_sigs(L):
     L.imr_engine_set_admission.argtypes = [vp, C.c_size_t]
     L.imr_engine_set_step_target.argtypes = [vp, C.c_double]
     L.imr_engine_set_schedule.argtypes = [vp, C.c_int]
+    L.imr_engine_set_autotune.argtypes = [vp, C.c_int, C.c_char_p]
 
 
 class Engine:
@@ -404,6 +407,12 @@ class Engine:
     def set_schedule(self, schedule: int):
         """SCHEDULE_GROUPED (default) or SCHEDULE_CHAINED step graphs."""
         _check(lib().imr_engine_set_schedule(self._h, schedule), "imr_engine_set_schedule")
+
+    def set_autotune(self, enable: bool = True, cache_path: str | None = None):
+        """Pick the step configuration per admitted set by timing real steps; cache in a file."""
+        _check(lib().imr_engine_set_autotune(self._h, 1 if enable else 0,
+                                             cache_path.encode() if cache_path else None),
+               "imr_engine_set_autotune")
 
     def set_step_target(self, ms: float):
         """Admit requests only while the predicted step time stays within `ms` (0: off)."""

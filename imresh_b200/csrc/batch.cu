@@ -34,6 +34,7 @@
 #include <chrono>
 #include <deque>
 #include <map>
+#include <string>
 #include <tuple>
 #include <vector>
 
@@ -124,6 +125,16 @@ struct Chain {
 };
 constexpr int kBranchStreams = 16;
 
+// Step configurations the tuner compares on real steps (all give the same
+// bits): the schedule, and the persistent grids at 100 % or 50 % of the
+// occupancy limit (fewer, longer-running CTAs overlap more copy with compute
+// when a class has few items per CTA).
+struct TuneCfg {
+    int schedule, grid_pct;
+};
+constexpr TuneCfg kTuneCands[] = {{0, 100}, {1, 100}, {0, 50}, {1, 50}};
+constexpr int kTuneN = 4;
+
 }  // namespace imr
 
 using namespace imr;
@@ -170,6 +181,17 @@ struct imr_engine {
     long steps = 0;
     int sms = 148;
     int schedule = 0;                 // IMR_SCHEDULE_GROUPED / IMR_SCHEDULE_CHAINED
+    int grid_pct = 100;               // persistent grids at this % of the occupancy limit
+    // online tuner: per admitted-set signature, run each candidate for one
+    // step, time it on the device, keep the fastest (ms per resident pixel)
+    bool tune = false;
+    std::string tune_path;            // cache file ("": memory only)
+    std::map<std::string, TuneCfg> tune_cache;
+    std::string tune_sig;             // signature of the set being run
+    int tune_next = -1;               // next candidate to launch (-1: settled)
+    long tune_step[kTuneN] = {};      // the step each candidate ran at
+    double tune_ms[kTuneN] = {};      // its measured ms per pixel (0: not yet)
+    long tune_explored = 0, tune_hits = 0;
     cudaStream_t bs[kBranchStreams] = {};
     cudaEvent_t ev_fork = nullptr, ev_join[kBranchStreams] = {};
     int inject_alloc_fail = 0;      // the next admissions whose allocation is made to fail
@@ -184,6 +206,7 @@ struct imr_engine {
     cudaEvent_t ev_t0[2] = {nullptr, nullptr}, ev_t1[2] = {nullptr, nullptr};
     size_t step_px[2] = {0, 0};
     double last_step_ms = 0.0;
+    double device_ms = 0.0;           // device time of all observed steps
 };
 
 #define CKE(call)                      \
@@ -373,7 +396,8 @@ static int launch_cycle(imr_engine *E, cudaStream_t s, const WorkList *L, std::v
     int rc;
     for (auto &g : rowg) {
         if (g.pipelined) {
-            if ((rc = launch_finish(g.rk, (int)g.items.size(), g.smem_fin, s, E->dj, L + g.list_base, nullptr)))
+            if ((rc = launch_finish(g.rk, (int)g.items.size(), g.smem_fin, s, E->dj, L + g.list_base, nullptr,
+                                    E->grid_pct)))
                 return rc;
         } else {
             g.rk.finish<<<loop_grid(E, (int)g.items.size()), g.rk.threads, g.smem_fin, s>>>(E->dj, L + g.list_base,
@@ -395,7 +419,8 @@ static int launch_cycle(imr_engine *E, cudaStream_t s, const WorkList *L, std::v
             if (g.pipelined) {
                 auto kf = i == 0 ? g.rk.p_hio_first : g.rk.p_hio;
                 const int sm = i == 0 ? g.rk.p_smem_first : g.rk.p_smem;
-                kf<<<persistent_grid((const void *)kf, g.rk.threads, sm, n), g.rk.threads, sm, s>>>(E->dj, Li);
+                kf<<<scaled_grid((const void *)kf, g.rk.threads, sm, n, E->grid_pct), g.rk.threads, sm, s>>>(E->dj,
+                                                                                                          Li);
             } else {
                 (i == 0 ? g.rk.hio_first : g.rk.hio)<<<loop_grid(E, n), g.rk.threads, g.smem, s>>>(E->dj, Li);
             }
@@ -406,7 +431,7 @@ static int launch_cycle(imr_engine *E, cudaStream_t s, const WorkList *L, std::v
             const WorkList *Li = L + g.list_base + 1 + i;
             const int n = g.hio_count[i];
             if (g.pipelined)
-                g.ck.p_col<<<persistent_grid((const void *)g.ck.p_col, g.ck.p_threads, g.ck.p_smem, n),
+                g.ck.p_col<<<scaled_grid((const void *)g.ck.p_col, g.ck.p_threads, g.ck.p_smem, n, E->grid_pct),
                              g.ck.p_threads, g.ck.p_smem, s>>>(E->dj, Li);
             else
                 g.ck.col<<<loop_grid(E, n), g.ck.threads, g.smem, s>>>(E->dj, Li);
@@ -453,6 +478,110 @@ static int launch_chain(imr_engine *E, cudaStream_t s, const WorkList *L, Chain 
     const int rc = launch_cycle(E, s, L, rg, cg, c.vb_base, c.vb.size(), &k);
     *kernels += k;
     return rc;
+}
+
+// ---- online tuner ----------------------------------------------------------
+// Signature of the admitted set: its kernel classes (row length, column
+// length, pipelined or not) with their job counts.
+static std::string set_signature(const std::vector<EJob *> &jobs)
+{
+    std::map<std::tuple<int, int, int, int>, int> n;
+    for (EJob *j : jobs) ++n[std::make_tuple((int)j->W, (int)j->H, j->S.p_rows ? 1 : 0, j->S.p_cols ? 1 : 0)];
+    std::string sig;
+    char buf[64];
+    for (auto &kv : n) {
+        snprintf(buf, sizeof(buf), "%dx%d%c%c*%d;", std::get<0>(kv.first), std::get<1>(kv.first),
+                 std::get<2>(kv.first) ? 'p' : 't', std::get<3>(kv.first) ? 'p' : 't', kv.second);
+        sig += buf;
+    }
+    return sig;
+}
+
+static void tune_load(imr_engine *E)
+{
+    E->tune_cache.clear();
+    if (E->tune_path.empty()) return;
+    FILE *f = fopen(E->tune_path.c_str(), "r");
+    if (!f) return;
+    char line[8192];
+    while (fgets(line, sizeof(line), f)) {
+        char *tab = strchr(line, '\t');
+        if (!tab) continue;
+        *tab = 0;
+        int sched = 0, pct = 100;
+        if (sscanf(tab + 1, "%d %d", &sched, &pct) == 2 && (sched == 0 || sched == 1) && pct > 0 && pct <= 100)
+            E->tune_cache[line] = TuneCfg{sched, pct};
+    }
+    fclose(f);
+}
+
+static void tune_store(imr_engine *E, const std::string &sig, const TuneCfg &c, double ms_per_mpx)
+{
+    E->tune_cache[sig] = c;
+    if (E->tune_path.empty()) return;
+    FILE *f = fopen(E->tune_path.c_str(), "a");
+    if (!f) return;
+    fprintf(f, "%s\t%d %d %.6f\n", sig.c_str(), c.schedule, c.grid_pct, ms_per_mpx);
+    fclose(f);
+}
+
+// Before a rebuild: a new set starts its exploration (or takes its cached
+// configuration); during exploration every step runs the next candidate.
+static void tune_before_step(imr_engine *E)
+{
+    if (!E->tune || E->active.empty()) return;
+    const std::string sig = set_signature(E->active);
+    if (sig != E->tune_sig) {
+        E->tune_sig = sig;
+        auto it = E->tune_cache.find(sig);
+        if (it != E->tune_cache.end()) {
+            E->tune_next = -1;
+            ++E->tune_hits;
+            if (E->schedule != it->second.schedule || E->grid_pct != it->second.grid_pct) E->dirty = true;
+            E->schedule = it->second.schedule;
+            E->grid_pct = it->second.grid_pct;
+            return;
+        }
+        E->tune_next = 0;
+        for (int c = 0; c < kTuneN; ++c) {
+            E->tune_step[c] = -1;
+            E->tune_ms[c] = 0.0;
+        }
+    }
+    if (E->tune_next >= 0 && E->tune_next < kTuneN) {
+        const TuneCfg &c = kTuneCands[E->tune_next];
+        if (E->schedule != c.schedule || E->grid_pct != c.grid_pct) E->dirty = true;
+        E->schedule = c.schedule;
+        E->grid_pct = c.grid_pct;
+    }
+}
+
+// After the launch of step n: note which candidate it ran.
+static void tune_after_launch(imr_engine *E, long n)
+{
+    if (!E->tune || E->tune_next < 0 || E->tune_next >= kTuneN) return;
+    E->tune_step[E->tune_next] = n;
+    ++E->tune_next;
+    ++E->tune_explored;
+}
+
+// When the device time of step m is known: record it; once every candidate
+// is timed, keep the fastest.
+static void tune_observe(imr_engine *E, long m, double ms_per_px)
+{
+    if (!E->tune || E->tune_next < 0) return;
+    for (int c = 0; c < kTuneN; ++c)
+        if (E->tune_step[c] == m) E->tune_ms[c] = ms_per_px;
+    for (int c = 0; c < kTuneN; ++c)
+        if (!(E->tune_ms[c] > 0)) return;
+    int best = 0;
+    for (int c = 1; c < kTuneN; ++c)
+        if (E->tune_ms[c] < E->tune_ms[best]) best = c;
+    E->tune_next = -1;
+    tune_store(E, E->tune_sig, kTuneCands[best], E->tune_ms[best] * 1e6);
+    if (E->schedule != kTuneCands[best].schedule || E->grid_pct != kTuneCands[best].grid_pct) E->dirty = true;
+    E->schedule = kTuneCands[best].schedule;
+    E->grid_pct = kTuneCands[best].grid_pct;
 }
 
 // Rebuild the work lists of the active set and the newly admitted jobs'
@@ -593,8 +722,10 @@ static int observe(imr_engine *E, const JobState *hs, long m)
         float ms = 0.f;
         if (E->step_px[q] && cudaEventElapsedTime(&ms, E->ev_t0[q], E->ev_t1[q]) == cudaSuccess) {
             E->last_step_ms = ms;
+            E->device_ms += ms;
             const double r = ms / (double)E->step_px[q];
             E->ms_per_px = E->ms_per_px > 0 ? 0.8 * E->ms_per_px + 0.2 * r : r;
+            tune_observe(E, m, r);
         }
         cudaGetLastError();
     }
@@ -794,6 +925,7 @@ int imr_engine_step(imr_engine *E)
         E->fresh.clear();
         return E->retiring.empty() ? IMR_SUCCESS : drain(E);
     }
+    tune_before_step(E);
     if (E->dirty && (rc = rebuild(E))) return rc;
     // column init of the newly admitted jobs, then one cycle of every active job
     const WorkList *L = E->d_lists;
@@ -811,6 +943,7 @@ int imr_engine_step(imr_engine *E)
     CKE(cudaGraphLaunch(E->gexec, E->s));
     CKE(cudaEventRecord(E->ev_t1[q], E->s));
     E->step_px[q] = E->active_px;
+    tune_after_launch(E, n);
     ++E->host_launches;
     E->launches += E->kernels_per_step;
     CKE(cudaMemcpyAsync(E->hst[q], E->dst, sizeof(JobState) * E->max_slots, cudaMemcpyDeviceToHost, E->s));
@@ -894,6 +1027,17 @@ int imr_engine_set_schedule(imr_engine *E, int schedule)
         E->schedule = schedule;
         E->dirty = true;
     }
+    return IMR_SUCCESS;
+}
+
+int imr_engine_set_autotune(imr_engine *E, int enable, const char *cache_path)
+{
+    if (!E) return IMR_ERR_INVALID_VALUE;
+    E->tune = enable != 0;
+    E->tune_path = cache_path ? cache_path : "";
+    E->tune_sig.clear();
+    E->tune_next = -1;
+    tune_load(E);
     return IMR_SUCCESS;
 }
 
@@ -1016,6 +1160,11 @@ int imr_engine_stats(imr_engine *E, imr_engine_info *st)
     st->resident_px = E->active_px;
     st->last_step_ms = E->last_step_ms;
     st->ms_per_mpx = E->ms_per_px * 1e6;
+    st->device_ms = E->device_ms;
+    st->schedule = E->schedule;
+    st->grid_pct = E->grid_pct;
+    st->tune_explored = E->tune_explored;
+    st->tune_cache_hits = E->tune_hits;
     return IMR_SUCCESS;
 }
 

@@ -338,11 +338,18 @@ int persistent_grid(const void *kernel, int threads, int smem, int items)
     return (int)(g < items ? g : items);
 }
 
+int scaled_grid(const void *kernel, int threads, int smem, int items, int grid_pct)
+{
+    const int g = persistent_grid(kernel, threads, smem, 1 << 30);   // the occupancy limit
+    const long want = std::max(1L, (long)g * grid_pct / 100);
+    return (int)std::min<long>(want, std::max(items, 1));
+}
+
 int launch_finish(const RowKernels &rk, int items, size_t smem_fin, cudaStream_t s, const JobDev *dj,
-                  const WorkList *L, float2 *dbg)
+                  const WorkList *L, float2 *dbg, int grid_pct)
 {
     if (rk.p_finish)
-        rk.p_finish<<<persistent_grid((const void *)rk.p_finish, rk.threads, rk.p_smem_fin, items), rk.threads,
+        rk.p_finish<<<scaled_grid((const void *)rk.p_finish, rk.threads, rk.p_smem_fin, items, grid_pct), rk.threads,
                       rk.p_smem_fin, s>>>(dj, L, dbg);
     else
         rk.finish<<<items, rk.threads, smem_fin, s>>>(dj, L, dbg);

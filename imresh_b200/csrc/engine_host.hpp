@@ -76,8 +76,11 @@ int fft_passes(float2 *d, int W, int H, int sign, int axes, const FftPlanDev &pr
 int persistent_grid(const void *kernel, int threads, int smem, int items);
 // Launch the once-per-cycle row pass over `items` row tiles: the pipelined
 // persistent kernel where the row length has one, else one CTA per tile.
+// grid_pct: the persistent grid at this percentage of the occupancy limit.
 int launch_finish(const RowKernels &rk, int items, size_t smem_fin, cudaStream_t s, const JobDev *dj,
-                  const WorkList *L, float2 *dbg);
+                  const WorkList *L, float2 *dbg, int grid_pct = 100);
+// Persistent grid scaled to grid_pct % of the occupancy limit (at least 1 CTA, at most `items`).
+int scaled_grid(const void *kernel, int threads, int smem, int items, int grid_pct);
 // 2D tensor map over a row-major [H][W] array of `elem`-byte elements with a
 // (box_w, box_h) box; returns false when the shape cannot be described.
 bool encode_tensor_map(CUtensorMap *map, const void *base, int W, int H, int elem, int box_w, int box_h);

@@ -330,6 +330,11 @@ typedef struct imr_engine_info {
     size_t resident_px;    /* their pixels                                   */
     double last_step_ms;   /* device time of the last step whose state was read */
     double ms_per_mpx;     /* step time per million resident pixels (running) */
+    double device_ms;      /* device time of all steps whose state was read  */
+    int schedule;          /* IMR_SCHEDULE_* in use                          */
+    int grid_pct;          /* persistent grids at this % of the occupancy limit */
+    long tune_explored;    /* steps the tuner ran to compare configurations  */
+    long tune_cache_hits;  /* admitted sets whose configuration came from the cache */
 } imr_engine_info;
 
 /* device_bytes: admission budget (0 = 80 % of the free device memory);
@@ -367,6 +372,16 @@ int imr_engine_cancel(imr_engine *engine, long long tag);
 #define IMR_SCHEDULE_GROUPED 0
 #define IMR_SCHEDULE_CHAINED 1
 int imr_engine_set_schedule(imr_engine *engine, int schedule);
+/* Online tuner of the step configuration.  For every admitted set (its
+ * kernel classes and their job counts) not seen before, the next steps run
+ * the candidate configurations -- the two schedules, persistent grids at 100 %
+ * and 50 % of the occupancy limit -- one step each; their device times per
+ * resident pixel are compared and the fastest is kept for the set and
+ * appended to `cache_path` (a text file, one line per set; NULL or "" keeps it
+ * in memory), which later engines load here, so a known set starts with its
+ * configuration.  Every candidate gives the same bits.  enable = 0 turns the
+ * tuner off (the configuration in use stays). */
+int imr_engine_set_autotune(imr_engine *engine, int enable, const char *cache_path);
 /* Bound on the work admitted at once: a pending request is admitted only
  * while the pixels (W*H) of all resident requests, its own included, stay
  * within max_active_pixels (0 = no bound: device memory alone decides), or

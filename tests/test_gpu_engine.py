@@ -211,3 +211,36 @@ def test_reference_examples_run_unchanged(cuda, tmp_path, name):
         pytest.skip("reference examples not built (oracle/Makefile examples)")
     r = subprocess.run([exe], capture_output=True, text=True, timeout=300, cwd=str(tmp_path))
     assert r.returncode == 0, r.stdout + r.stderr
+
+
+def test_autotuner_explores_once_then_uses_its_cache(cuda, tmp_path):
+    """The engine's tuner runs each candidate step configuration (two
+    schedules x two persistent-grid sizes) for one step of a new admitted
+    set, keeps the fastest, and writes it to its cache file; a second engine
+    with the same cache and the same set starts with that configuration and
+    explores nothing.  Every configuration gives the same bits."""
+    p = imr.Params(10, FLT_MIN, 0.9, 0.04, 0.2, 3.0, 0.01, 4)
+    shapes = [(128, 128), (256, 192), (192, 256), (256, 256), (128, 384), (384, 128)]
+    inputs = [data.make_modulus(data.BlobSpec(W, H, 10, 0.15 * min(W, H), (1.0, 3.0), (0.3, 1.0), 1e8), 13, i)[0]
+              for i, (W, H) in enumerate(shapes)]
+    cache = str(tmp_path / "tune.txt")
+    runs = []
+    for attempt in range(2):
+        eng = imr.Engine()
+        eng.set_autotune(True, cache)
+        for i, M in enumerate(inputs):
+            eng.submit(M, p, tag=i)
+        eng.run()
+        res = {r["tag"]: r["out"] for r in eng.poll()}
+        runs.append((res, eng.info()))
+        eng.close()
+    (res0, info0), (res1, info1) = runs
+    assert info0["tune_explored"] == 4 and info0["tune_cache_hits"] == 0, info0
+    assert info1["tune_explored"] == 0 and info1["tune_cache_hits"] == 1, info1
+    assert (info1["schedule"], info1["grid_pct"]) == (info0["schedule"], info0["grid_pct"])
+    lines = open(cache).read().strip().splitlines()
+    assert len(lines) == 1 and "\t" in lines[0]
+    for i, M in enumerate(inputs):
+        alone = _alone(M, p)[0]
+        np.testing.assert_array_equal(res0[i], alone)
+        np.testing.assert_array_equal(res1[i], alone)
