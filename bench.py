@@ -25,12 +25,15 @@ translation, next to the reference FP32 path's own distance to FP64 -- the
   plain_256        256x256, 60 blobs, 64 x 20: GPU recon/s (device, e2e), the
                    reference's CPU shrinkWrap timed on a FULL reconstruction
   batched_uneven   512 reconstructions, W, H in {128..512}, 64 x 20: the
-                   batched engine (one graph launch per cycle step) vs the
-                   plain path per request
+                   batched engine (one graph launch per cycle step, step
+                   configuration chosen by its online tuner, cached in
+                   $IMR_TUNE_CACHE or ~/.cache/imresh_b200/engine_tune.txt)
+                   vs the plain path per request
   large_4096       4096x4096, 1500 blobs, 32 x 20: the FP32 path and the
                    split-precision tensor-core column passes (BF16 / FP16 hi+lo)
-  served_stream    Poisson arrivals, sides log-uniform 64..2048, stop at 1e-5
-                   or 128 cycles: recon/s, latency p50/p99, device bytes
+  served_stream    Poisson arrivals at 70 % of the measured capacity, sides
+                   log-uniform 64..2048, stop at 1e-5 or 128 cycles: recon/s,
+                   latency p50/p99, device bytes
 The CPU baseline is the reference's own CPU shrinkWrap (compiled from its
 sources over the project FFT, oracle/_ref), timed after all GPU work with
 the host otherwise idle; the accuracy runs of the FP64 restatement come last.
@@ -424,21 +427,29 @@ def run_large_4096(args, flush, stream):
     return res, {"M": M, "obj": obj, "out1": keep}
 
 
-def run_served(n_req: int, rate_hz: float, seed: int = 4, max_side: int = 2048, max_active_px: int = 0,
-               schedule: int = 0, step_target_ms: float = 0.0):
-    """Serving stream: n_req requests with Poisson arrivals at rate_hz;
-    W, H log-uniform integers in [64, max_side] (any length: mixed radix or
-    Bluestein), 0.5-3 blobs per 1000 px^2, Poisson 1e6-1e9 photons; each
-    request stops at error 1e-5 or 128 cycles.  Requests are admitted by the
-    engine between steps as device memory (and the admitted-work bound, when
-    set) allows; latency = arrival -> result in host memory."""
-    import imresh_b200 as imr
+def served_inputs(n_req: int, seed: int = 4, max_side: int = 2048):
+    """The serving stream's requests: W, H log-uniform integers in [64,
+    max_side] (any length: mixed radix or Bluestein), 0.5-3 blobs per 1000
+    px^2, Poisson 1e6-1e9 photons."""
     from imresh_b200 import data
     specs = data.cfg4_specs(n_req, seed=seed)
     for sp in specs:
         sp.width = min(sp.width, max_side)
         sp.height = min(sp.height, max_side)
-    inputs = [data.make_modulus(sp, seed=seed, index=i)[0] for i, sp in enumerate(specs)]
+    return [data.make_modulus(sp, seed=seed, index=i)[0] for i, sp in enumerate(specs)]
+
+
+def run_served(n_req: int, rate_hz: float, seed: int = 4, max_side: int = 2048, max_active_px: int = 0,
+               schedule: int = 0, step_target_ms: float = 0.0, inputs=None):
+    """Serving stream: n_req requests (served_inputs) with Poisson arrivals at
+    rate_hz; each request stops at error 1e-5 or 128 cycles.  Requests are
+    admitted by the engine between steps as device memory (and the
+    admitted-work bound, when set) allows; latency = arrival -> result in
+    host memory."""
+    import imresh_b200 as imr
+    if inputs is None:
+        inputs = served_inputs(n_req, seed, max_side)
+    inputs = inputs[:n_req]
     rng = np.random.default_rng([seed, 7])
     arrivals = np.cumsum(rng.exponential(1.0 / rate_hz, n_req))
     prm = imr.Params(128, 1e-5, 0.9, 0.04, 0.2, 3.0, 0.01, 20)
@@ -471,16 +482,34 @@ def run_served(n_req: int, rate_hz: float, seed: int = 4, max_side: int = 2048, 
     info = eng.info()
     eng.close()
     p50, p99 = _lat_stats(lat)
-    return {"workload": f"{n_req} requests, Poisson arrivals at {rate_hz} /s, sides log-uniform "
+    px = sum(M.size for M in inputs)
+    return {"workload": f"{n_req} requests, Poisson arrivals at {rate_hz:.2f} /s, sides log-uniform "
                         f"64..{max_side}, stop at 1e-5 or 128 cycles, seed {seed}",
             "recon_per_s": n_req / wall, "latency_p50_ms": p50, "latency_p99_ms": p99,
             "latency_max_ms": float(np.max(lat)), "offered_rate_hz": rate_hz,
             "peak_resident": peak_active, "device_bytes_peak": info["device_bytes_peak"],
+            "mean_request_px": px / n_req,
             "max_active_px": max_active_px or None, "step_target_ms": step_target_ms or None,
             "schedule": "chained" if schedule else "grouped",
             "mean_cycles": float(np.mean(cycles)), "steps": info["steps"], "kernels": info["launches"],
             "host_launches": info["host_launches"], "graph_builds": info["graph_builds"],
-            "graph_updates": info["graph_updates"]}
+            "graph_updates": info["graph_updates"], "device_seconds": info["device_ms"] / 1e3,
+            "wall_seconds": wall}
+
+
+def run_served_default(n_req: int, load: float = 0.7):
+    """The served stream as the default bench runs it: the capacity first (the
+    first 150 requests all at once), then n_req requests with Poisson arrivals
+    at `load` x that capacity; both on the chained schedule with a 20 ms
+    step-time admission target."""
+    inputs = served_inputs(n_req)
+    cap = run_served(min(150, n_req), 1e4, schedule=1, step_target_ms=20.0, inputs=inputs)
+    rate = load * cap["recon_per_s"]
+    r = run_served(n_req, rate, schedule=1, step_target_ms=20.0, inputs=inputs)
+    r["capacity_recon_per_s"] = cap["recon_per_s"]
+    r["capacity_sample"] = "first 150 requests of the stream, all submitted at once"
+    r["load"] = load
+    return r
 
 
 # ---------------------------------------------------------------- reference arm
@@ -615,7 +644,8 @@ def run_ours(args, rank, world, local_rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded Gaussian-blob objects, Poisson noise)",
-        "config": dict(main_config(world), hio_iterations_per_s=value * N_CYCLES * N_HIO),
+        "config": main_config(world),
+        "hio_iterations_per_s": value * N_CYCLES * N_HIO,
         "e2e": {"value": e2e_value, "unit": "recon/s", "h2d_bytes_per_step": 4 * W * H,
                 "d2h_bytes_per_step": 4 * W * H,
                 "api": "imr_cuda_shrink_wrap (drop-in for cudaShrinkWrap), pinned host buffer"},
@@ -642,7 +672,10 @@ def run_ours(args, rank, world, local_rank):
     wl = {}
     keep = {}
     wl["plain_256"], keep["plain_256"] = run_plain_256(args, flush, stream)
-    wl["batched_uneven"], keep["batched"] = run_batched()
+    tune_cache = os.environ.get("IMR_TUNE_CACHE") or os.path.join(os.path.expanduser("~"), ".cache",
+                                                                      "imresh_b200", "engine_tune.txt")
+    os.makedirs(os.path.dirname(tune_cache), exist_ok=True)
+    wl["batched_uneven"], keep["batched"] = run_batched(tune_cache=tune_cache)
     wl["large_4096"], keep["large"] = run_large_4096(args, flush, stream)
     # four cycles of the headline workload on the GPU, for the FP64 comparison
     p4 = imr.Plan(W, H, imr.Params(4, imr.FLT_MIN, PARAMS["beta"], PARAMS["cut_auto"], PARAMS["cut"],
@@ -651,7 +684,7 @@ def run_ours(args, rank, world, local_rank):
     _, errs4 = p4.stats()
     p4.close()
     if args.serve_requests:
-        wl["served_stream"] = run_served(args.serve_requests, args.rate, max_active_px=args.max_active_px)
+        wl["served_stream"] = run_served_default(args.serve_requests)
 
     if not args.no_cpu_baseline:
         # CPU legs, the host otherwise idle: the timed baselines first
@@ -704,6 +737,14 @@ def run_ours(args, rank, world, local_rank):
             al = accuracy(o, res["4096x1_f64"][0], res["4096x1_f32"][0], kl["obj"])
             al["scope"] = "1 cycle x 1 HIO (before HIO's amplification; the full run is out of reach of the CPU)"
             wl["large_4096"][name]["accuracy"] = al
+        bu = wl["batched_uneven"]
+        wl["engine_vs_plain"] = {
+            "recon_per_s_ratio": bu["speedup_engine_vs_plain"],
+            "at_equal_error": f"engine results bit-identical to the plain FP32 path ({bu['engine_equals_plain_bitwise']} "
+                              "sampled); aligned rel. L2 to FP64 of a batch job "
+                              f"{bu['accuracy']['rel_l2_vs_fp64']:.3g} vs the reference FP32 path's "
+                              f"{bu['accuracy']['reference_fp32_rel_l2_vs_fp64']:.3g}",
+            "split_precision_vs_fp32": wl["large_4096"]["split_vs_fp32_recon_ratio"]}
         wl["equal_error"] = (
             "HIO amplifies rounding ~2x per iteration: past a few cycles any FP32 run, the reference's "
             "included, is as far from the FP64 run as unrelated images; 'equal error' = the GPU's aligned "
@@ -721,12 +762,16 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--only-main", action="store_true", help="only the headline workload")
     ap.add_argument("--serve-requests", type=int, default=400, metavar="N",
-                    help="requests of the served stream in the default run (0: skip)")
-    ap.add_argument("--rate", type=float, default=7.0, help="serving arrival rate, requests/s")
+                    help="requests of the served stream in the default run, at 70 %% of its measured "
+                         "capacity (0: skip)")
+    ap.add_argument("--rate", type=float, default=7.0, help="--serve: arrival rate, requests/s")
     ap.add_argument("--max-active-px", type=int, default=0,
                     help="served stream: bound on the pixels of the admitted requests (0: memory only)")
     ap.add_argument("--serve", type=int, default=0, metavar="N",
                     help="only run the serving stream with N requests and print its JSON")
+    ap.add_argument("--schedule", type=int, default=0, help="--serve: 0 grouped, 1 chained step graphs")
+    ap.add_argument("--step-target", type=float, default=0.0,
+                    help="--serve: admission bound from the measured step time, ms (0: off)")
     ap.add_argument("--ncu-case", type=int, default=0, metavar="N",
                     help="run one NxN reconstruction (1 cycle x 3 HIO) and exit: a small case for ncu")
     ap.add_argument("--ncu-prec", type=int, default=0,
@@ -749,7 +794,8 @@ def main():
     if args.serve:
         import torch
         torch.cuda.set_device(0)
-        print(json.dumps(run_served(args.serve, args.rate, max_active_px=args.max_active_px)), flush=True)
+        print(json.dumps(run_served(args.serve, args.rate, max_active_px=args.max_active_px,
+                                    schedule=args.schedule, step_target_ms=args.step_target)), flush=True)
         return
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))

@@ -244,3 +244,39 @@ def test_autotuner_explores_once_then_uses_its_cache(cuda, tmp_path):
         alone = _alone(M, p)[0]
         np.testing.assert_array_equal(res0[i], alone)
         np.testing.assert_array_equal(res1[i], alone)
+
+
+def test_admission_bounds_keep_results_and_the_bound(cuda):
+    """A pixel bound admits requests only while the resident pixels stay
+    within it (or one request when nothing runs); a step-time target admits
+    by the measured cost per pixel.  Neither changes any result."""
+    inputs = _inputs()[:8]
+    bound = 256 * 256 + 192 * 256
+    eng = imr.Engine()
+    eng.set_admission(bound)
+    for i, (M, p) in enumerate(inputs):
+        eng.submit(M, p, tag=i)
+    peak = 0
+    while True:
+        info = eng.info()
+        if info["pending"] == 0 and info["active"] == 0:
+            break
+        assert info["resident_px"] <= bound or info["resident"] == 1, info
+        peak = max(peak, info["resident_px"])
+        eng.step()
+    res = {r["tag"]: r for r in eng.poll()}
+    eng.close()
+    assert len(res) == len(inputs) and peak > 0
+    eng = imr.Engine()
+    eng.set_schedule(imr.SCHEDULE_CHAINED)
+    eng.set_step_target(2.0)
+    for i, (M, p) in enumerate(inputs):
+        eng.submit(M, p, tag=i)
+    eng.run()
+    res2 = {r["tag"]: r for r in eng.poll()}
+    assert eng.info()["ms_per_mpx"] > 0
+    eng.close()
+    for i, (M, p) in enumerate(inputs):
+        alone = _alone(M, p)[0]
+        np.testing.assert_array_equal(res[i]["out"], alone)
+        np.testing.assert_array_equal(res2[i]["out"], alone)
