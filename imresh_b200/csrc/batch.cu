@@ -196,6 +196,7 @@ struct imr_engine {
     cudaEvent_t ev_fork = nullptr, ev_join[kBranchStreams] = {};
     int inject_alloc_fail = 0;      // the next admissions whose allocation is made to fail
     long alloc_failures = 0;
+    size_t reserved = 0;            // bytes the engine's pool has been grown to
     size_t max_active_px = 0;       // bound on the pixels of the resident requests (0: none)
     size_t active_px = 0;
     // admission by measured step time: every step's graph is timed on the
@@ -205,6 +206,7 @@ struct imr_engine {
     double ms_per_px = 0.0;
     cudaEvent_t ev_t0[2] = {nullptr, nullptr}, ev_t1[2] = {nullptr, nullptr};
     size_t step_px[2] = {0, 0};
+    double step_launch_ms[2] = {0.0, 0.0};   // host time of the step's graph launch call
     double last_step_ms = 0.0;
     double device_ms = 0.0;           // device time of all observed steps
 };
@@ -268,8 +270,44 @@ static void finish_now(imr_engine *E, EJob *j, int status)
     E->done.push_back(j);
 }
 
+// Grow the pool's reserve in one piece before a batch of admissions: the
+// pool keeps what it is given (release threshold: never), so the arenas of
+// the batch are then carved from memory it already holds instead of each
+// admission growing the pool on its own (one driver mapping per arena cost
+// 0.2-0.7 s for 512 admissions).
+static void reserve_for(imr_engine *E)
+{
+    size_t want = 0, px = E->active_px;
+    int slots = (int)E->free_slots.size();
+    bool idle = E->active.empty() && E->fresh.empty();
+    for (EJob *j : E->pending) {   // the requests admit() is about to take, by the same tests
+        if (slots == 0) break;
+        const size_t jp = (size_t)j->W * j->H;
+        if (E->used + want + j->S.bytes > E->budget && !idle) break;
+        if (E->max_active_px && px + jp > E->max_active_px && !idle) break;
+        if (E->target_step_ms > 0 && E->ms_per_px > 0 && (double)(px + jp) * E->ms_per_px > E->target_step_ms &&
+            !idle)
+            break;
+        want += (j->S.bytes + 511) / 512 * 512;
+        px += jp;
+        --slots;
+        idle = false;
+    }
+    if (want == 0 || E->used + want <= E->reserved) return;
+    const size_t grow = E->used + want - E->reserved;
+    if (E->inject_alloc_fail > 0) return;   // the injected failures are the admissions' own
+    void *tmp = nullptr;
+    if (cudaMallocFromPoolAsync(&tmp, grow, E->pool, E->s) == cudaSuccess) {
+        cudaFreeAsync(tmp, E->s);
+        E->reserved += grow;
+    } else {
+        cudaGetLastError();   // not fatal: each admission then allocates (and may fail) on its own
+    }
+}
+
 static int admit(imr_engine *E)
 {
+    reserve_for(E);
     while (!E->pending.empty() && !E->free_slots.empty()) {
         EJob *j = E->pending.front();
         const bool idle = E->active.empty() && E->fresh.empty();
@@ -526,7 +564,11 @@ static void tune_store(imr_engine *E, const std::string &sig, const TuneCfg &c, 
 }
 
 // Before a rebuild: a new set starts its exploration (or takes its cached
-// configuration); during exploration every step runs the next candidate.
+// configuration); during exploration each candidate runs for kTuneRuns steps
+// and the last of them is timed (the first launch of a new graph carries
+// one-time costs).
+constexpr int kTuneRuns = 2;
+
 static void tune_before_step(imr_engine *E)
 {
     if (!E->tune || E->active.empty()) return;
@@ -548,8 +590,8 @@ static void tune_before_step(imr_engine *E)
             E->tune_ms[c] = 0.0;
         }
     }
-    if (E->tune_next >= 0 && E->tune_next < kTuneN) {
-        const TuneCfg &c = kTuneCands[E->tune_next];
+    if (E->tune_next >= 0 && E->tune_next < kTuneN * kTuneRuns) {
+        const TuneCfg &c = kTuneCands[E->tune_next / kTuneRuns];
         if (E->schedule != c.schedule || E->grid_pct != c.grid_pct) E->dirty = true;
         E->schedule = c.schedule;
         E->grid_pct = c.grid_pct;
@@ -559,8 +601,8 @@ static void tune_before_step(imr_engine *E)
 // After the launch of step n: note which candidate it ran.
 static void tune_after_launch(imr_engine *E, long n)
 {
-    if (!E->tune || E->tune_next < 0 || E->tune_next >= kTuneN) return;
-    E->tune_step[E->tune_next] = n;
+    if (!E->tune || E->tune_next < 0 || E->tune_next >= kTuneN * kTuneRuns) return;
+    if (E->tune_next % kTuneRuns == kTuneRuns - 1) E->tune_step[E->tune_next / kTuneRuns] = n;
     ++E->tune_next;
     ++E->tune_explored;
 }
@@ -687,6 +729,8 @@ static int rebuild(imr_engine *E)
             return IMR_ERR_CUDA;
         }
     }
+    // upload now, so the first launch of the new graph does not carry it
+    CKE(cudaGraphUpload(E->gexec, E->s));
     if (E->graph) cudaGraphDestroy(E->graph);
     E->graph = g;
     E->kernels_per_step = kernels;
@@ -725,7 +769,9 @@ static int observe(imr_engine *E, const JobState *hs, long m)
             E->device_ms += ms;
             const double r = ms / (double)E->step_px[q];
             E->ms_per_px = E->ms_per_px > 0 ? 0.8 * E->ms_per_px + 0.2 * r : r;
-            tune_observe(E, m, r);
+            // the tuner weighs a configuration by the device time plus the host
+            // time its graph launch takes (a larger graph costs the host more)
+            tune_observe(E, m, (ms + E->step_launch_ms[q]) / (double)E->step_px[q]);
         }
         cudaGetLastError();
     }
@@ -940,7 +986,9 @@ int imr_engine_step(imr_engine *E)
     E->fresh.clear();
     const int q = (int)(n & 1);
     CKE(cudaEventRecord(E->ev_t0[q], E->s));
+    const double tl = now_ms();
     CKE(cudaGraphLaunch(E->gexec, E->s));
+    E->step_launch_ms[q] = now_ms() - tl;
     CKE(cudaEventRecord(E->ev_t1[q], E->s));
     E->step_px[q] = E->active_px;
     tune_after_launch(E, n);

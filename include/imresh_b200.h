@@ -375,8 +375,9 @@ int imr_engine_set_schedule(imr_engine *engine, int schedule);
 /* Online tuner of the step configuration.  For every admitted set (its
  * kernel classes and their job counts) not seen before, the next steps run
  * the candidate configurations -- the two schedules, persistent grids at 100 %
- * and 50 % of the occupancy limit -- one step each; their device times per
- * resident pixel are compared and the fastest is kept for the set and
+ * and 50 % of the occupancy limit -- two steps each; the times per resident
+ * pixel of their second steps (device time plus the host time of the graph
+ * launch) are compared and the fastest is kept for the set and
  * appended to `cache_path` (a text file, one line per set; NULL or "" keeps it
  * in memory), which later engines load here, so a known set starts with its
  * configuration.  Every candidate gives the same bits.  enable = 0 turns the

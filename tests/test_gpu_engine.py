@@ -215,11 +215,11 @@ def test_reference_examples_run_unchanged(cuda, tmp_path, name):
 
 def test_autotuner_explores_once_then_uses_its_cache(cuda, tmp_path):
     """The engine's tuner runs each candidate step configuration (two
-    schedules x two persistent-grid sizes) for one step of a new admitted
-    set, keeps the fastest, and writes it to its cache file; a second engine
+    schedules x two persistent-grid sizes) for two steps of a new admitted
+    set, times the second, keeps the fastest, and writes it to its cache file; a second engine
     with the same cache and the same set starts with that configuration and
     explores nothing.  Every configuration gives the same bits."""
-    p = imr.Params(10, FLT_MIN, 0.9, 0.04, 0.2, 3.0, 0.01, 4)
+    p = imr.Params(14, FLT_MIN, 0.9, 0.04, 0.2, 3.0, 0.01, 4)
     shapes = [(128, 128), (256, 192), (192, 256), (256, 256), (128, 384), (384, 128)]
     inputs = [data.make_modulus(data.BlobSpec(W, H, 10, 0.15 * min(W, H), (1.0, 3.0), (0.3, 1.0), 1e8), 13, i)[0]
               for i, (W, H) in enumerate(shapes)]
@@ -235,7 +235,7 @@ def test_autotuner_explores_once_then_uses_its_cache(cuda, tmp_path):
         runs.append((res, eng.info()))
         eng.close()
     (res0, info0), (res1, info1) = runs
-    assert info0["tune_explored"] == 4 and info0["tune_cache_hits"] == 0, info0
+    assert info0["tune_explored"] == 8 and info0["tune_cache_hits"] == 0, info0   # 4 candidates x 2 steps
     assert info1["tune_explored"] == 0 and info1["tune_cache_hits"] == 1, info1
     assert (info1["schedule"], info1["grid_pct"]) == (info0["schedule"], info0["grid_pct"])
     lines = open(cache).read().strip().splitlines()
