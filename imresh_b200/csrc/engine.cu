@@ -274,6 +274,7 @@ static ColKernels col_set()
             k.fft_tc[0][1] = k_col_tc<N, T, kPrecBf16x3, 2>;
             k.fft_tc[1][0] = k_col_tc<N, T, kPrecFp16x3, 1>;
             k.fft_tc[1][1] = k_col_tc<N, T, kPrecFp16x3, 2>;
+            k.p_smem_tc = pcol_tc_smem<N, T>();
         }
         return k;
     } else if constexpr (N >= 16 && is_pow2(N))
@@ -585,6 +586,7 @@ struct imr_plan {
     int g_row_first = 0, g_row = 0, g_col = 0;
     WorkList *Lrow = nullptr, *Lcol = nullptr, *Lvb = nullptr;   // device
     int prec = 0;   // column pass: 0 FP32, 1 BF16 hi+lo tensor cores, 2 FP16 hi+lo tensor cores
+    int g_col_tc = 0;
 };
 
 // The pipelined column pass of the plan's precision.
@@ -611,7 +613,8 @@ static int plan_launch_cycle(imr_plan *P, cudaStream_t s)
             (i == 0 ? rk.hio_first : rk.hio)<<<J.n_row_tiles, rk.threads, P->smem_row, s>>>(P->dj, P->Lrow);
         }
         if (P->p_cols)
-            plan_col_kernel(P)<<<P->g_col, ck.p_threads, ck.p_smem, s>>>(P->dj, P->Lcol);
+            plan_col_kernel(P)<<<P->prec ? P->g_col_tc : P->g_col, ck.p_threads,
+                                 P->prec ? ck.p_smem_tc : ck.p_smem, s>>>(P->dj, P->Lcol);
         else
             ck.col<<<J.n_col_tiles, ck.threads, P->smem_col, s>>>(P->dj, P->Lcol);
     }
@@ -1010,7 +1013,8 @@ static cudaError_t profile_replay(imr_plan *P, int iters, bool split, cudaStream
                 P->rk.hio<<<J.n_row_tiles, P->rk.threads, P->smem_row, cs>>>(P->dj, P->Lrow);
             if (split) cudaEventRecordWithFlags(ev[k++], cs, cudaEventRecordExternal);
             if (P->p_cols)
-                plan_col_kernel(P)<<<P->g_col, P->ck.p_threads, P->ck.p_smem, cs>>>(P->dj, P->Lcol);
+                plan_col_kernel(P)<<<P->prec ? P->g_col_tc : P->g_col, P->ck.p_threads,
+                                     P->prec ? P->ck.p_smem_tc : P->ck.p_smem, cs>>>(P->dj, P->Lcol);
             else
                 P->ck.col<<<J.n_col_tiles, P->ck.threads, P->smem_col, cs>>>(P->dj, P->Lcol);
             if (split || i == iters - 1) cudaEventRecordWithFlags(ev[k++], cs, cudaEventRecordExternal);
@@ -1090,6 +1094,9 @@ int imr_plan_set_precision(imr_plan *P, int precision)
     }
     if (precision == P->prec) return IMR_SUCCESS;
     P->prec = precision;
+    if (precision != IMR_PREC_FP32)
+        P->g_col_tc = persistent_grid((const void *)P->ck.p_col_tc[precision - 1], P->ck.p_threads, P->ck.p_smem_tc,
+                                      P->hj.n_col_tiles);
     CK(cudaDeviceSynchronize());
     return plan_capture(P);
 }
@@ -1131,12 +1138,12 @@ int imr_fft2d_split(void *d_data, unsigned W, unsigned H, int sign, int precisio
     CK(cudaMemcpyAsync(dj, &J, sizeof(JobDev), cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(dl, &wl, sizeof(WorkList), cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(dst, 0, sizeof(JobState), s));
-    const int grid = persistent_grid((const void *)kcol, ck.p_threads, ck.p_smem, J.n_col_tiles);
+    const int grid = persistent_grid((const void *)kcol, ck.p_threads, ck.p_smem_tc, J.n_col_tiles);
     if (sign < 0) {
         if ((rc = fft_passes((float2 *)d_data, (int)W, (int)H, -1, 1, pr, pc, s))) return rc;
-        kcol<<<grid, ck.p_threads, ck.p_smem, s>>>(dj, dl);
+        kcol<<<grid, ck.p_threads, ck.p_smem_tc, s>>>(dj, dl);
     } else {
-        kcol<<<grid, ck.p_threads, ck.p_smem, s>>>(dj, dl);
+        kcol<<<grid, ck.p_threads, ck.p_smem_tc, s>>>(dj, dl);
         if ((rc = fft_passes((float2 *)d_data, (int)W, (int)H, +1, 1, pr, pc, s))) return rc;
     }
     CK(cudaGetLastError());

@@ -66,6 +66,7 @@ struct ColKernels {
     // column transforms; null where the length has none
     void (*p_col_tc[2])(const JobDev *, const WorkList *);
     void (*fft_tc[2][2])(const JobDev *, const WorkList *);   // [precision][0 forward, 1 inverse]
+    int p_smem_tc;   // their dynamic shared memory
 };
 RowKernels row_kernels(int N);
 ColKernels col_kernels(int N);

@@ -216,7 +216,7 @@ __device__ __forceinline__ void tc_pass16(float2 *buf, const float2 *__restrict_
             float2 v = LOAD ? buf[IN::at(T.b, j + p * Q)] : y[mt][i];
             if constexpr (NS > 1) {
                 const int k = j % NS;
-                float2 w = __ldg(tw + ((k * STEP * p) & (N - 1)));
+                float2 w = tw[(k * STEP * p) & (N - 1)];   // the shared-memory copy of the table
                 if (S > 0) w.y = -w.y;
                 v = cmul(v, w);
             }
@@ -239,6 +239,11 @@ __device__ __forceinline__ void tc_pass16(float2 *buf, const float2 *__restrict_
         __syncthreads();
     }
 }
+
+// Dynamic shared memory of k_col_tc: the stages of k_col_p16 and the
+// length-N twiddle table.
+template <int N, int NBT>
+__host__ __device__ constexpr int pcol_tc_smem() { return pcol16_smem<N, NBT>() + N * 8; }
 
 // Column pass with split-precision tensor-core stages.  MODE 0: forward
 // FFT, modulus projection, inverse FFT (the shrink-wrap / HIO column pass);
@@ -282,10 +287,11 @@ __global__ void __launch_bounds__(pcol16_threads(N, NBT), 1) k_col_tc(const JobD
     Dft16B<PREC> B;
     B.init(lane);
     RegTw16<N> rtw;   // twiddles of the CUDA-core last pass
-    const float2 *tw = nullptr;
+    float2 *tw = reinterpret_cast<float2 *>(stages + NST * STAGE);   // the table, copied once per CTA
     if (item < n_items) {
-        tw = jobs[walk.at(item).job].pcol.tw;
-        if constexpr (!LAST16) rtw.load(tw, l);
+        const float2 *gtw = jobs[walk.at(item).job].pcol.tw;
+        for (int i = threadIdx.x; i < N; i += pcol16_threads(N, NBT)) tw[i] = __ldg(gtw + i);
+        if constexpr (!LAST16) rtw.load(gtw, l);
     }
     int it_next = n_items;
     if (threadIdx.x == 0) {

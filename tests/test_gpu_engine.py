@@ -280,3 +280,26 @@ def test_admission_bounds_keep_results_and_the_bound(cuda):
         alone = _alone(M, p)[0]
         np.testing.assert_array_equal(res[i]["out"], alone)
         np.testing.assert_array_equal(res2[i]["out"], alone)
+
+
+def test_chained_schedule_with_more_classes_than_branch_streams(cuda):
+    """More (row kernel, column kernel) classes than the graph's 16 branch
+    streams: chains share streams in turn and every result still equals the
+    reconstruction alone."""
+    # widths and heights of distinct kernel classes: powers of two and 3*2^k,
+    # a runtime-radix length (100) and Bluestein lengths of three work sizes
+    shapes = [(W, H) for W in (64, 128, 192, 97, 131) for H in (64, 256, 100, 263)]
+    p = imr.Params(2, FLT_MIN, 0.9, 0.04, 0.2, 3.0, 0.01, 3)
+    inputs = [data.make_modulus(data.BlobSpec(W, H, 6, 0.15 * min(W, H), (1.0, 2.0), (0.3, 1.0), 1e8), 17, i)[0]
+              for i, (W, H) in enumerate(shapes)]
+    eng = imr.Engine()
+    eng.set_schedule(imr.SCHEDULE_CHAINED)
+    for i, M in enumerate(inputs):
+        eng.submit(M, p, tag=i)
+    eng.step()
+    assert eng.info()["kernels_per_step"] >= 17 * (2 + 2 * 3)
+    eng.run()
+    res = {r["tag"]: r["out"] for r in eng.poll()}
+    eng.close()
+    for i, M in enumerate(inputs):
+        np.testing.assert_array_equal(res[i], _alone(M, p)[0])
