@@ -290,7 +290,8 @@ def run_plain_256(args, flush, stream):
     return r, {"M": M, "obj": obj, "out": out, "errors": errs}
 
 
-def run_batched(n_jobs: int = 512, plain_sample: int = 64, schedule: int = 0, tune_cache: str | None = None):
+def run_batched(n_jobs: int = 512, plain_sample: int = 64, schedule: int = 0, tune_cache: str | None = None,
+                cycles_per_step: int = 1):
     """The uneven batch: n_jobs reconstructions, W and H each from
     {128,192,256,384,512}, 20-200 blobs, Poisson 1e7-1e9 photons, seed 2,
     64 cycles x 20 HIO.  Served by the batched engine (all jobs submitted at
@@ -315,6 +316,7 @@ def run_batched(n_jobs: int = 512, plain_sample: int = 64, schedule: int = 0, tu
     eng.close()
     eng = imr.Engine()
     eng.set_schedule(schedule)
+    eng.set_cycles_per_step(cycles_per_step)
     if tune_cache is not None:
         eng.set_autotune(True, tune_cache)
     t0 = time.perf_counter()
@@ -362,6 +364,7 @@ def run_batched(n_jobs: int = 512, plain_sample: int = 64, schedule: int = 0, tu
         "engine_graph_builds": info["graph_builds"] + info["graph_updates"],
         "engine_device_seconds": info["device_ms"] / 1e3,
         "engine_schedule": "chained" if info["schedule"] else "grouped", "engine_grid_pct": info["grid_pct"],
+        "engine_cycles_per_step": info["cycles_per_step"],
         "engine_tuner": {"explored_steps": info["tune_explored"], "cache_hits": info["tune_cache_hits"]}
                         if tune_cache is not None else None,
         "plain_recon_per_s": plain_sample / dt_plain, "plain_sample_jobs": plain_sample,
@@ -773,7 +776,8 @@ def main():
     ap.add_argument("--step-target", type=float, default=0.0,
                     help="--serve: admission bound from the measured step time, ms (0: off)")
     ap.add_argument("--ncu-case", type=int, default=0, metavar="N",
-                    help="run one NxN reconstruction (1 cycle x 3 HIO) and exit: a small case for ncu")
+                    help="run one NxN reconstruction (1 cycle x 3 HIO) of the headline recipe scaled to N "
+                         "and exit: a small case for ncu")
     ap.add_argument("--ncu-prec", type=int, default=0,
                     help="column-pass precision of the ncu case (0 FP32, 1 BF16 hi+lo, 2 FP16 hi+lo)")
     args = ap.parse_args()
@@ -782,7 +786,9 @@ def main():
         import imresh_b200 as imr
         from imresh_b200 import data
         n = args.ncu_case
-        M, _ = data.make_modulus(data.BlobSpec(n, n, 60, 0.15 * n, (2.0, 2.0), (0.5, 1.0), None), 0)
+        # the headline's blob density, radius and Poisson noise, scaled to N x N
+        M, _ = data.make_modulus(data.BlobSpec(n, n, max(1, 400 * n * n // 2048 ** 2), 300.0 * n / 2048,
+                                               (1.5, 3.0), (0.3, 1.0), 1e9), 0)
         plan = imr.Plan(n, n, imr.Params(1, imr.FLT_MIN, 0.9, 0.04, 0.2, 3.0, 0.01, 3))
         plan.set_precision(args.ncu_prec)
         d_m = torch.from_numpy(M).cuda()

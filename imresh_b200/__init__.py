@@ -296,7 +296,7 @@ class CEngineInfo(C.Structure):
                 ("graph_updates", C.c_long), ("alloc_failures", C.c_long), ("resident", C.c_int),
                 ("resident_px", C.c_size_t), ("last_step_ms", C.c_double), ("ms_per_mpx", C.c_double),
                 ("device_ms", C.c_double), ("schedule", C.c_int), ("grid_pct", C.c_int),
-                ("tune_explored", C.c_long), ("tune_cache_hits", C.c_long)]
+                ("tune_explored", C.c_long), ("tune_cache_hits", C.c_long), ("cycles_per_step", C.c_int)]
 
 
 def _engine_sigs(L):
@@ -319,6 +319,7 @@ def _engine_sigs(L):
     L.imr_engine_set_step_target.argtypes = [vp, C.c_double]
     L.imr_engine_set_schedule.argtypes = [vp, C.c_int]
     L.imr_engine_set_autotune.argtypes = [vp, C.c_int, C.c_char_p]
+    L.imr_engine_set_cycles_per_step.argtypes = [vp, C.c_int]
 
 
 class Engine:
@@ -417,6 +418,10 @@ class Engine:
     def set_step_target(self, ms: float):
         """Admit requests only while the predicted step time stays within `ms` (0: off)."""
         _check(lib().imr_engine_set_step_target(self._h, float(ms)), "imr_engine_set_step_target")
+
+    def set_cycles_per_step(self, cycles: int):
+        """Shrink-wrap cycles captured into one step's graph (1..256; default 1)."""
+        _check(lib().imr_engine_set_cycles_per_step(self._h, int(cycles)), "imr_engine_set_cycles_per_step")
 
     def inject_alloc_failures(self, count: int):
         """Make the device allocations of the next `count` admissions fail (tests)."""

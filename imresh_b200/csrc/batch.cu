@@ -75,6 +75,7 @@ struct EJob {
     float last_error = 0.f;
     int status = IMR_SUCCESS;
     long admit_step = -1;       // its state was set before this step's state copy: older copies are stale
+    long cycles_launched = 0;   // cycles queued for it so far (a request ends after n_cycles + 1)
     long copy_step = -1;        // retiring: its result copy precedes this step's status copy
     int staging = -1;           // retiring: index of its pinned staging chunk (-1: direct copy)
     size_t staging_off = 0;     // its place in that chunk
@@ -182,6 +183,7 @@ struct imr_engine {
     int sms = 148;
     int schedule = 0;                 // IMR_SCHEDULE_GROUPED / IMR_SCHEDULE_CHAINED
     int grid_pct = 100;               // persistent grids at this % of the occupancy limit
+    int cycles_per_step = 1;          // shrink-wrap cycles captured into one step's graph
     // online tuner: per admitted-set signature, run each candidate for one
     // step, time it on the device, keep the fastest (ms per resident pixel)
     bool tune = false;
@@ -376,6 +378,7 @@ static int admit(imr_engine *E)
             CKE(cudaMemcpyAsync(j->J.mask, d + N * 20, N, cudaMemcpyHostToDevice, E->s));
             CKE(cudaMemcpyAsync(j->J.errors, d + N * 21, (size_t)h->n_err * 4, cudaMemcpyHostToDevice, E->s));
             CKE(cudaStreamSynchronize(E->s));
+            j->cycles_launched = h->st.cycle;   // the cycle it continues with
             std::vector<char>().swap(j->resume);
         }
         j->admit_step = E->steps;   // the slot's previous state is in every older state copy
@@ -687,14 +690,16 @@ static int rebuild(imr_engine *E)
     long kernels = 0;
     CKE(cudaStreamBeginCapture(E->cs, cudaStreamCaptureModeThreadLocal));
     if (!chained) {
-        rc = launch_cycle(E, E->cs, E->d_lists, rowg, colg, vb_base, vb.size(), &kernels);
+        for (int c = 0; c < E->cycles_per_step && rc == IMR_SUCCESS; ++c)
+            rc = launch_cycle(E, E->cs, E->d_lists, rowg, colg, vb_base, vb.size(), &kernels);
     } else {
         // one branch per chain (chains beyond the branch streams share them in turn)
         cudaError_t e = cudaEventRecord(E->ev_fork, E->cs);
         const int nb = std::min((int)chains.size(), kBranchStreams);
         for (int b = 0; b < nb && e == cudaSuccess; ++b) e = cudaStreamWaitEvent(E->bs[b], E->ev_fork, 0);
         for (size_t c = 0; c < chains.size() && e == cudaSuccess && rc == IMR_SUCCESS; ++c)
-            rc = launch_chain(E, E->bs[c % kBranchStreams], E->d_lists, chains[c], &kernels);
+            for (int k = 0; k < E->cycles_per_step && rc == IMR_SUCCESS; ++k)
+                rc = launch_chain(E, E->bs[c % kBranchStreams], E->d_lists, chains[c], &kernels);
         for (int b = 0; b < nb && e == cudaSuccess; ++b) {
             e = cudaEventRecord(E->ev_join[b], E->bs[b]);
             if (e == cudaSuccess) e = cudaStreamWaitEvent(E->cs, E->ev_join[b], 0);
@@ -966,6 +971,19 @@ int imr_engine_step(imr_engine *E)
         CKE(cudaEventSynchronize(E->ev_st[q]));
         if ((rc = observe(E, E->hst[q], n - 2))) return rc;
     }
+    if (n > 0 && E->pending.empty() && !E->active.empty()) {
+        // every cycle of every running request is queued and nothing waits:
+        // read the last step's state instead of queueing steps that would only
+        // find them stopped
+        bool all = true;
+        for (EJob *j : E->active) all = all && j->cycles_launched >= (long)j->J.n_cycles + 1;
+        if (all) {
+            const int q = (int)((n - 1) & 1);
+            CKE(cudaEventSynchronize(E->ev_st[q]));
+            if (n - 1 > E->synced_step && (rc = observe(E, E->hst[q], n - 1))) return rc;
+            if (E->active.empty()) return drain(E);
+        }
+    }
     if ((rc = admit(E))) return rc;
     if (E->active.empty()) {   // nothing to run: hand over what is still in flight
         E->fresh.clear();
@@ -992,6 +1010,7 @@ int imr_engine_step(imr_engine *E)
     CKE(cudaEventRecord(E->ev_t1[q], E->s));
     E->step_px[q] = E->active_px;
     tune_after_launch(E, n);
+    for (EJob *j : E->active) j->cycles_launched += E->cycles_per_step;
     ++E->host_launches;
     E->launches += E->kernels_per_step;
     CKE(cudaMemcpyAsync(E->hst[q], E->dst, sizeof(JobState) * E->max_slots, cudaMemcpyDeviceToHost, E->s));
@@ -1073,6 +1092,17 @@ int imr_engine_set_schedule(imr_engine *E, int schedule)
     if (!E || (schedule != IMR_SCHEDULE_GROUPED && schedule != IMR_SCHEDULE_CHAINED)) return IMR_ERR_INVALID_VALUE;
     if (schedule != E->schedule) {
         E->schedule = schedule;
+        E->dirty = true;
+    }
+    return IMR_SUCCESS;
+}
+
+int imr_engine_set_cycles_per_step(imr_engine *E, int cycles)
+{
+    if (!E || cycles < 1 || cycles > 256) return IMR_ERR_INVALID_VALUE;
+    if (cycles != E->cycles_per_step) {
+        E->cycles_per_step = cycles;
+        E->ms_per_px = 0;   // the running step cost per pixel was for the old step length
         E->dirty = true;
     }
     return IMR_SUCCESS;
@@ -1213,6 +1243,7 @@ int imr_engine_stats(imr_engine *E, imr_engine_info *st)
     st->grid_pct = E->grid_pct;
     st->tune_explored = E->tune_explored;
     st->tune_cache_hits = E->tune_hits;
+    st->cycles_per_step = E->cycles_per_step;
     return IMR_SUCCESS;
 }
 

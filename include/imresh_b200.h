@@ -335,6 +335,7 @@ typedef struct imr_engine_info {
     int grid_pct;          /* persistent grids at this % of the occupancy limit */
     long tune_explored;    /* steps the tuner ran to compare configurations  */
     long tune_cache_hits;  /* admitted sets whose configuration came from the cache */
+    int cycles_per_step;   /* shrink-wrap cycles in one step's graph         */
 } imr_engine_info;
 
 /* device_bytes: admission budget (0 = 80 % of the free device memory);
@@ -344,9 +345,12 @@ int imr_engine_create(imr_engine **engine, size_t device_bytes, int max_jobs, vo
  * request is admitted, h_out (W*H floats) until its result is polled. */
 int imr_engine_submit(imr_engine *engine, const float *h_modulus, float *h_out, unsigned W,
                       unsigned H, const imr_params *params, long long tag);
-/* Retire what had finished two steps ago, admit, launch one cycle of every
- * active reconstruction.  Returns once the step is queued (it waits only for
- * the step before the previous one). */
+/* Retire what had finished two steps ago, admit, launch one step (one cycle,
+ * or imr_engine_set_cycles_per_step's count) of every active reconstruction.
+ * Returns once the step is queued (it waits only for the step before the
+ * previous one).  When every cycle of every running request has been queued
+ * and nothing is pending, it waits for the last step instead and retires
+ * them. */
 int imr_engine_step(imr_engine *engine);
 /* Step until nothing is pending, running or being copied out. */
 int imr_engine_run(imr_engine *engine);
@@ -398,6 +402,13 @@ int imr_engine_set_admission(imr_engine *engine, size_t max_active_pixels);
  * is then about its cycle count times the target, plus its wait in the
  * queue. */
 int imr_engine_set_step_target(imr_engine *engine, double target_step_ms);
+/* Shrink-wrap cycles captured into one step's graph (1..256, default 1).
+ * More cycles per step mean fewer host launches and state read-backs per
+ * cycle, and later retirement and admission (a finished request waits for
+ * the end of its step; the others skip the rest of it on the device).  The
+ * step-time target then applies to a step of that many cycles.  Results are
+ * bit-identical for every count.  No counterpart in the reference. */
+int imr_engine_set_cycles_per_step(imr_engine *engine, int cycles);
 /* Host-side fault injection for tests of the failure paths: the device
  * allocations of the next `count` admissions fail as if the device were out
  * of memory.  A request whose allocation fails waits in the queue while

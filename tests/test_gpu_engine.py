@@ -58,6 +58,29 @@ def test_mixed_batch_equals_alone(cuda):
     eng.close()
 
 
+def test_several_cycles_per_step(cuda):
+    """Four cycles per step graph: the same bits as one request alone, about a
+    quarter of the steps, and no step queued after the last request's final
+    cycle (the engine waits for that step's state instead)."""
+    inputs = _inputs()
+    eng = imr.Engine()
+    eng.set_cycles_per_step(4)
+    for i, (M, p) in enumerate(inputs):
+        eng.submit(M, p, tag=i)
+    eng.run()
+    res = {r["tag"]: r for r in eng.poll()}
+    info = eng.info()
+    eng.close()
+    assert info["cycles_per_step"] == 4
+    longest = max(p.n_cycles for _, p in inputs) + 1
+    assert info["steps"] <= (longest + 3) // 4 + 1, info
+    assert sorted(res) == list(range(len(inputs)))
+    for i, (M, p) in enumerate(inputs):
+        alone, n = _alone(M, p)
+        assert res[i]["status"] == 0 and res[i]["cycles_done"] == n == p.n_cycles
+        np.testing.assert_array_equal(res[i]["out"], alone)
+
+
 def test_admission_under_memory_budget(cuda):
     inputs = [(data.make_modulus(data.BlobSpec(256, 256, 10, 38.0, (1.5, 2.5), (0.5, 1.0), None), 9, i)[0],
                imr.Params(2, FLT_MIN, 0.9, 0.04, 0.2, 3.0, 0.01, 3)) for i in range(6)]
