@@ -265,7 +265,7 @@ static ColKernels col_set()
     if constexpr (N >= 128 && N <= 4096 && is_pow2(N)) {   // 16 values per thread in the pipelined pass
         constexpr int T = pcol16_nbt(N);
         ColKernels k{k_col_r<N>, k_col_init_r<N>, k_fft_cols_r<-1, N>, k_fft_cols_r<+1, N>,
-                     rcol_nb(N), rcol_threads(N), rcol_smem(N), k_col_p16<N, T>, pcol16_smem<N, T>(),
+                     rcol_nb(N), rcol_threads(N), rcol_smem(N), k_col_p16<N, T, false>, pcol16_smem<N, T>(),
                      pcol_box_rows(N), 0, pcol16_threads(N, T), 0, T, 1};
         if constexpr (N >= 256) {   // split-precision tensor-core variants
             k.p_col_tc[0] = k_col_tc<N, T, kPrecBf16x3, 0>;
@@ -276,6 +276,7 @@ static ColKernels col_set()
             k.fft_tc[1][1] = k_col_tc<N, T, kPrecFp16x3, 2>;
             k.p_smem_tc = pcol_tc_smem<N, T>();
         }
+        if constexpr (T >= 4) k.p_col_split = k_col_p16<N, T, true>;   // half tiles of >= 2 columns (16-byte TMA rows)
         return k;
     } else if constexpr (N >= 16 && is_pow2(N))
         return ColKernels{k_col_r<N>, k_col_init_r<N>, k_fft_cols_r<-1, N>, k_fft_cols_r<+1, N>,
@@ -337,6 +338,18 @@ int persistent_grid(const void *kernel, int threads, int smem, int items)
     }
     const long g = (long)occ.first * occ.second;
     return (int)(g < items ? g : items);
+}
+
+// A persistent column pass runs one tile per CTA at a time.  When the tiles
+// fill at most half of the resident CTAs (256^2: 16 tiles, 512^2: 32, on 148
+// SMs) every tile runs as two half tiles on two CTAs (bit-identical results):
+// measured 5.6 -> 5.1 us at 256^2 and 8.8 -> 6.9 us at 512^2.  Beyond that a
+// half tile, at ~79 % of a whole tile's time, loses: splitting each CTA's first
+// and last tile at 2048^2 took the pass from 33.3 to 37.6 us, and all tiles at
+// 1024^2 (two rounds of halves) from 9.8 to 12.7 us.
+int col_split(int n_tiles, int g_max)
+{
+    return (n_tiles > 0 && 2 * n_tiles <= g_max) ? n_tiles : 0;
 }
 
 int scaled_grid(const void *kernel, int threads, int smem, int items, int grid_pct)
@@ -484,6 +497,7 @@ int ensure_kernel_attributes()
         if (e == cudaSuccess && r.p_hio_fix) e = allow_smem(r.p_hio_fix);
         if (e == cudaSuccess && r.p_finish) e = allow_smem(r.p_finish);
         if (e == cudaSuccess && c.p_col) e = allow_smem(c.p_col);
+        if (e == cudaSuccess && c.p_col_split) e = allow_smem(c.p_col_split);
         for (int pr = 0; pr < 2; ++pr) {
             if (e == cudaSuccess && c.p_col_tc[pr]) e = allow_smem(c.p_col_tc[pr]);
             for (int d = 0; d < 2; ++d)
@@ -730,6 +744,7 @@ void job_bind(JobDev &J, JobShape &S, char *a, JobState *st)
         }
         J.use_tma_cols = S.p_cols ? 1 : 0;
         if (S.p_cols && S.ck.p_mt) J.Mt = (const float *)(a + S.oMt);
+        S.p_half = S.p_cols && S.ck.p_col_split && encode_tensor_map(&J.tmXh, J.X, J.W, J.H, 8, S.ck.p_nb / 2, br);
     }
 }
 
@@ -888,9 +903,18 @@ int imr_plan_create(imr_plan **out, unsigned W, unsigned H, const imr_params *pa
                                          J.n_row_tiles);
         P->g_row = persistent_grid((const void *)P->rk.p_hio, P->rk.threads, P->rk.p_smem, J.n_row_tiles);
     }
-    if (P->p_cols)
-        P->g_col = persistent_grid((const void *)P->ck.p_col, P->ck.p_threads, P->ck.p_smem, J.n_col_tiles);
-    const WorkList lists[3] = {{nullptr, J.n_row_tiles}, {nullptr, J.n_col_tiles}, {nullptr, J.n_vb_tiles}};
+    int n_split = 0;
+    if (P->p_cols) {
+        int g_max = persistent_grid((const void *)P->ck.p_col, P->ck.p_threads, P->ck.p_smem, 1 << 30);
+        if (S.p_half && col_split(J.n_col_tiles, g_max)) {   // the half-tile variant of the pass
+            P->ck.p_col = P->ck.p_col_split;
+            g_max = persistent_grid((const void *)P->ck.p_col, P->ck.p_threads, P->ck.p_smem, 1 << 30);
+            n_split = col_split(J.n_col_tiles, g_max);
+        }
+        P->g_col = std::min(g_max, J.n_col_tiles + n_split);
+    }
+    const WorkList lists[3] = {{nullptr, J.n_row_tiles, 0}, {nullptr, J.n_col_tiles, n_split},
+                               {nullptr, J.n_vb_tiles, 0}};
     e = cudaMemcpy(P->Lrow, lists, sizeof(lists), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = job_upload(J, S, a, P->dj, 0) ? cudaErrorUnknown : cudaSuccess;
     if (e == cudaSuccess) e = cudaDeviceSynchronize();

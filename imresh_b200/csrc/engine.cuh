@@ -56,6 +56,7 @@ constexpr int kModeHio = 1;   // fixed support, random initial phase
 struct alignas(64) JobDev {
     CUtensorMap tmX;    // X as W x H 8-byte elements, box (cpc, rows)
     CUtensorMap tmM;    // M as W x H floats, box (cpc, rows)
+    CUtensorMap tmXh;   // X as tmX with box (cpc / 2, rows): half tiles of the column pass
     int use_tma_cols;   // 1: column pass reads tiles through tmX / tmM
     int mode;           // kModeShrinkWrap / kModeHio
     int W, H;
@@ -93,9 +94,14 @@ struct WorkItem {
 };
 
 // A launch's items, in device memory.  items == nullptr: job 0, tiles 0..n-1.
+// n_split (items == nullptr, pipelined 16-value column pass only): tiles
+// 0..n_split-1 run as two half-width items each, the first halves before all
+// other items and the second halves after them (with n_split = n: every tile
+// as two halves, on twice as many CTAs).
 struct WorkList {
     const WorkItem *items;
     int n;
+    int n_split;
 };
 
 }  // namespace imr

@@ -67,6 +67,8 @@ struct ColKernels {
     void (*p_col_tc[2])(const JobDev *, const WorkList *);
     void (*fft_tc[2][2])(const JobDev *, const WorkList *);   // [precision][0 forward, 1 inverse]
     int p_smem_tc;   // their dynamic shared memory
+    void (*p_col_split)(const JobDev *, const WorkList *);   // p_col running WorkList::n_split
+                                                              // tiles as half tiles (JobDev::tmXh), or null
 };
 RowKernels row_kernels(int N);
 ColKernels col_kernels(int N);
@@ -82,6 +84,10 @@ int launch_finish(const RowKernels &rk, int items, size_t smem_fin, cudaStream_t
                   const WorkList *L, float2 *dbg, int grid_pct = 100);
 // Persistent grid scaled to grid_pct % of the occupancy limit (at least 1 CTA, at most `items`).
 int scaled_grid(const void *kernel, int threads, int smem, int items, int grid_pct);
+// WorkList::n_split of a persistent column launch of n_tiles tiles with at
+// most g_max CTAs resident (its grid: min(g_max, n_tiles + n_split)): every
+// tile when their halves fit the resident CTAs, else none.
+int col_split(int n_tiles, int g_max);
 // 2D tensor map over a row-major [H][W] array of `elem`-byte elements with a
 // (box_w, box_h) box; returns false when the shape cannot be described.
 bool encode_tensor_map(CUtensorMap *map, const void *base, int W, int H, int elem, int box_w, int box_h);
@@ -91,6 +97,7 @@ struct JobShape {
     RowKernels rk{};
     ColKernels ck{};
     bool p_rows = false, p_cols = false;
+    bool p_half = false;   // JobDev::tmXh encoded: the column pass may run half tiles
     size_t smem_row = 0, smem_fin = 0, smem_col = 0;
     size_t bytes = 0;   // arena bytes (JobState not included)
     size_t oX = 0, oG = 0, oM = 0, oMt = 0, oHB = 0, oVB = 0, oOut = 0, oMask = 0, oW = 0, oT = 0, oEP = 0, oErr = 0;

@@ -157,6 +157,74 @@ __device__ __forceinline__ void dft16(float2 *v)
     }
 }
 
+// The twiddle W16^(n2 k1) of element (n2, k1) of dft16's 4 x 4 step, by the
+// same expression dft16 uses for it (identity for n2 = 0 or k1 = 0).
+template <int S, int N2, int K1>
+__device__ __forceinline__ float2 dft16_tw(float2 y)
+{
+    const float c1 = 0.92387953251128675613f, s1 = 0.38268343236508977173f;   // cos, sin(pi/8)
+    const float h = 0.70710678118654752440f;
+    if constexpr (N2 == 0 || K1 == 0) return y;
+    else if constexpr (N2 * K1 == 1) return cmul(y, make_float2(c1, S * s1));
+    else if constexpr (N2 * K1 == 2) return make_float2(h * (y.x - S * y.y), h * (S * y.x + y.y));
+    else if constexpr (N2 * K1 == 3) return cmul(y, make_float2(s1, S * c1));
+    else if constexpr (N2 * K1 == 4) return mul_si<S>(y);
+    else if constexpr (N2 * K1 == 6) return make_float2(h * (-y.x - S * y.y), h * (S * y.x - y.y));
+    else return cmul(y, make_float2(-c1, -S * s1));   // 9
+}
+
+// dft16 split over two threads, H = 0 or 1: the thread holds u[j] = v[2j + H]
+// of dft16's v and ends holding the outputs v'[2j + H].  Part A: the DFT-4s
+// over n1 of rows n2 = H and H + 2 (inputs 4 n1 + n2 = 2j + H); their values in
+// the other parity's columns k1 = 1 - H, 3 - H go to the partner through `out`
+// (4 slots, `stride` apart) before twiddling.  Part B (after a barrier): the
+// partner's rows at columns k1 = H, H + 2 come from `in`; every element of
+// those columns is twiddled here, in the thread that sums it, as dft16 does,
+// and the DFT-4s over n2 give the outputs k1 + 4 k2 = 2j + H.
+template <int S, int H>
+__device__ __forceinline__ void dft16_half_a(const float2 (&u)[8], float2 (&ya)[4], float2 (&yb)[4], float2 *out,
+                                             int stride)
+{
+    ya[0] = u[0]; ya[1] = u[2]; ya[2] = u[4]; ya[3] = u[6];   // row n2 = H
+    yb[0] = u[1]; yb[1] = u[3]; yb[2] = u[5]; yb[3] = u[7];   // row n2 = H + 2
+    dft4<S>(ya);
+    dft4<S>(yb);
+    out[0] = ya[1 - H];
+    out[stride] = ya[3 - H];
+    out[2 * stride] = yb[1 - H];
+    out[3 * stride] = yb[3 - H];
+}
+template <int S, int H, int T>
+__device__ __forceinline__ void dft16_half_col(float2 (&u)[8], const float2 (&ya)[4], const float2 (&yb)[4],
+                                               float2 pa, float2 pb)
+{
+    constexpr int K1 = H + 2 * T;
+    float2 b[4];
+    if constexpr (H == 0) {
+        b[0] = ya[K1];
+        b[1] = dft16_tw<S, 1, K1>(pa);
+        b[2] = dft16_tw<S, 2, K1>(yb[K1]);
+        b[3] = dft16_tw<S, 3, K1>(pb);
+    } else {
+        b[0] = pa;
+        b[1] = dft16_tw<S, 1, K1>(ya[K1]);
+        b[2] = dft16_tw<S, 2, K1>(pb);
+        b[3] = dft16_tw<S, 3, K1>(yb[K1]);
+    }
+    dft4<S>(b);
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2) u[T + 2 * k2] = b[k2];
+}
+template <int S, int H>
+__device__ __forceinline__ void dft16_half_b(float2 (&u)[8], const float2 (&ya)[4], const float2 (&yb)[4],
+                                             const float2 *in, int stride)
+{
+    // the partner's rows n2 = 1 - H (pa) and 3 - H (pb) at columns H, H + 2
+    const float2 pa0 = in[0], pa1 = in[stride], pb0 = in[2 * stride], pb1 = in[3 * stride];
+    dft16_half_col<S, H, 0>(u, ya, yb, pa0, pb0);
+    dft16_half_col<S, H, 1>(u, ya, yb, pa1, pb1);
+}
+
 template <int S>
 __device__ __forceinline__ void dft3(float2 *v)
 {

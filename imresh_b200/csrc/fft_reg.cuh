@@ -502,6 +502,122 @@ __device__ __forceinline__ void reg16_fft(float2 (&v)[16], float2 *buf, int b, i
     reg16_passes<N, LAYOUT, S, 0, 1>(v, buf, b, l, tw);
 }
 
+// ---- half of each 16-value sequence per thread (half tiles) --------------------
+// Two threads share a sequence position l: thread h (0 or 1) holds v[2j + h],
+// j = 0..7, of the 16-value form and performs the operations reg16_passes
+// performs on those values, so the pair's results are reg16_fft's bit for bit.
+// A radix-16 butterfly trades four values with the partner through `mid`
+// (dft16_half_a / dft16_half_b; 8 * npairs values, `pair` indexing the
+// thread's (b, l)); the butterflies i of the smaller radices use values of one
+// parity (i + q*BPT = i mod 2), so thread h takes i = h, h + 2, ...  h must be
+// uniform over each warp; every barrier is in code that all threads run.
+
+// twiddle_pow<16, S> on the values of parity H (the same products)
+template <int S, int H>
+__device__ __forceinline__ void twiddle_pow16_half(float2 (&u)[8], const float2 (&p)[4])
+{
+    float2 w1 = p[0], w2 = p[1], w4 = p[2], w8 = p[3];
+    asm volatile("" : "+f"(w1.x), "+f"(w1.y), "+f"(w2.x), "+f"(w2.y), "+f"(w4.x), "+f"(w4.y), "+f"(w8.x),
+                 "+f"(w8.y));
+    if (S > 0) {
+        w1.y = -w1.y;
+        w2.y = -w2.y;
+        w4.y = -w4.y;
+        w8.y = -w8.y;
+    }
+    const float2 w3 = cmul(w1, w2);
+    float2 pw[8] = {make_float2(1.f, 0.f), w1, w2, w3, w4, cmul(w1, w4), cmul(w2, w4), cmul(w3, w4)};
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const int q = 2 * j + H;
+        if (q == 0) continue;
+        if (q < 8) u[j] = cmul(u[j], pw[q]);
+        else if (q == 8) u[j] = cmul(u[j], w8);
+        else u[j] = cmul(u[j], cmul(pw[q - 8], w8));
+    }
+}
+
+template <int N, class LAYOUT, int S, int P, int NS>
+__device__ __forceinline__ void reg16h_passes(float2 (&v)[8], float2 *buf, float2 *mid, int b, int l, int h,
+                                              int pair, int npairs, const RegTw16<N> &tw)
+{
+    constexpr RadixList L = reg16_radix_list(N);
+    if constexpr (P < L.n) {
+        constexpr int R = L.r[P];
+        constexpr int BPT = 16 / R;
+        constexpr int HB = BPT / 2 > 0 ? BPT / 2 : 1;   // butterflies per thread (R < 16)
+        constexpr int Q = N / 16;
+        constexpr int off = tw16_slots_upto(N, P);
+        int kk[HB];
+        if constexpr (R == 16) {
+            kk[0] = l % NS;
+            if constexpr (NS > 1) {
+                if (h) twiddle_pow16_half<S, 1>(v, tw.w[off]);
+                else twiddle_pow16_half<S, 0>(v, tw.w[off]);
+            }
+            float2 ya[4], yb[4];
+            if (h) dft16_half_a<S, 1>(v, ya, yb, mid + 4 * npairs + pair, npairs);
+            else dft16_half_a<S, 0>(v, ya, yb, mid + pair, npairs);
+            __syncthreads();
+            if (h) dft16_half_b<S, 1>(v, ya, yb, mid + pair, npairs);
+            else dft16_half_b<S, 0>(v, ya, yb, mid + 4 * npairs + pair, npairs);
+        } else {
+#pragma unroll
+            for (int t = 0; t < HB; ++t) {
+                const int i = 2 * t + h;
+                const int j = l + i * Q;
+                const int k = j % NS;
+                kk[t] = k;
+                float2 u[R];
+#pragma unroll
+                for (int q = 0; q < R; ++q) u[q] = v[t + q * HB];
+                if constexpr (NS > 1) {
+                    if constexpr (Q % NS == 0) {
+                        twiddle_pow<R, S>(u, tw.w[off]);
+                    } else {
+                        float2 p[4];
+#pragma unroll
+                        for (int e = 0; e < 4; ++e) p[e] = h ? tw.w[off + 2 * t + 1][e] : tw.w[off + 2 * t][e];
+                        twiddle_pow<R, S>(u, p);
+                    }
+                }
+                dftR<R, S>(u);
+#pragma unroll
+                for (int q = 0; q < R; ++q) v[t + q * HB] = u[q];
+            }
+        }
+        if constexpr (P + 1 < L.n) {
+            __syncthreads();   // earlier reads of buf are complete
+            if constexpr (R == 16) {
+                const int base = (l - kk[0]) * 16 + kk[0];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) buf[LAYOUT::at(b, base + (2 * j + h) * NS)] = v[j];
+            } else {
+#pragma unroll
+                for (int t = 0; t < HB; ++t) {
+                    const int j = l + (2 * t + h) * Q;
+                    const int base = (j - kk[t]) * R + kk[t];
+#pragma unroll
+                    for (int q = 0; q < R; ++q) buf[LAYOUT::at(b, base + q * NS)] = v[t + q * HB];
+                }
+            }
+            __syncthreads();
+#pragma unroll
+            for (int j = 0; j < 8; ++j) v[j] = buf[LAYOUT::at(b, l + (2 * j + h) * Q)];
+            reg16h_passes<N, LAYOUT, S, P + 1, NS * R>(v, buf, mid, b, l, h, pair, npairs, tw);
+        }
+    }
+}
+
+// reg16_fft on the values of parity h (see above); `mid` holds 8 * npairs values
+template <int N, class LAYOUT, int S>
+__device__ __forceinline__ void reg16h_fft(float2 (&v)[8], float2 *buf, float2 *mid, int b, int l, int h, int pair,
+                                           int npairs, const RegTw16<N> &tw)
+{
+    static_assert(is_pow2(N) && N >= 128 && N <= 4096, "16-value FFT length: 2^k, 128..4096");
+    reg16h_passes<N, LAYOUT, S, 0, 1>(v, buf, mid, b, l, h, pair, npairs, tw);
+}
+
 // shared memory (bytes) a register-FFT kernel needs
 __host__ __device__ constexpr int reg_smem_bytes(int N, int NB) { return 2 * NB * (N + N / 8) * 8; }
 

@@ -260,9 +260,17 @@ int imr_hio_plan_create(imr_hio_plan **out, unsigned W, unsigned H, unsigned nCy
     P->smem_col = S.smem_col;
     if (P->p_rows)
         P->g_row = persistent_grid((const void *)P->rk.p_hio_fix, P->rk.threads, P->rk.p_smem, J.n_row_tiles);
-    if (P->p_cols)
-        P->g_col = persistent_grid((const void *)P->ck.p_col, P->ck.p_threads, P->ck.p_smem, J.n_col_tiles);
-    const WorkList lists[2] = {{nullptr, J.n_row_tiles}, {nullptr, J.n_col_tiles}};
+    int n_split = 0;
+    if (P->p_cols) {
+        int g_max = persistent_grid((const void *)P->ck.p_col, P->ck.p_threads, P->ck.p_smem, 1 << 30);
+        if (S.p_half && col_split(J.n_col_tiles, g_max)) {   // the half-tile variant of the pass
+            P->ck.p_col = P->ck.p_col_split;
+            g_max = persistent_grid((const void *)P->ck.p_col, P->ck.p_threads, P->ck.p_smem, 1 << 30);
+            n_split = col_split(J.n_col_tiles, g_max);
+        }
+        P->g_col = std::min(g_max, J.n_col_tiles + n_split);
+    }
+    const WorkList lists[2] = {{nullptr, J.n_row_tiles, 0}, {nullptr, J.n_col_tiles, n_split}};
     e = cudaMemcpy(P->Lrow, lists, sizeof(lists), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = job_upload(J, S, a, P->dj, 0) ? cudaErrorUnknown : cudaSuccess;
     if (e == cudaSuccess) e = cudaHostAlloc((void **)&P->h_stop, 2 * sizeof(int), cudaHostAllocDefault);

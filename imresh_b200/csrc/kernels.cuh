@@ -2118,7 +2118,23 @@ template <int N, int NBT>
 __host__ __device__ constexpr int pcol16_smem() { return 128 + pcol16_stages<N, NBT>() * pcol16_stage_bytes<N, NBT>(); }
 __host__ __device__ constexpr int pcol16_min_blocks(int N, int NBT) { return NBT * N / 16 <= 256 ? 2 : 1; }
 
-template <int N, int NBT>
+// Item v of a column launch with n tiles of which the first S run as halves
+// (WorkList::n_split): v < S is half 0 of tile v, S <= v < n tile v whole,
+// n <= v < n + S half 1 of tile v - n.
+struct ColItem {
+    int tile, half;   // half: -1 the whole tile, else 0 / 1
+};
+__device__ __forceinline__ ColItem col_item(int v, int n, int S)
+{
+    if (v < S) return ColItem{v, 0};
+    if (v < n) return ColItem{v, -1};
+    return ColItem{v - n, 1};
+}
+
+// SPLIT: the variant that runs WorkList::n_split tiles as half tiles (plans
+// whose tiles fill at most half of the resident CTAs); the other keeps the
+// registers and code of whole tiles alone.
+template <int N, int NBT, bool SPLIT>
 __global__ void __launch_bounds__(pcol16_threads(N, NBT), pcol16_min_blocks(N, NBT))
 k_col_p16(const JobDev *jobs, const WorkList *L)
 {
@@ -2128,20 +2144,32 @@ k_col_p16(const JobDev *jobs, const WorkList *L)
     constexpr int BR = pcol_box_rows(N);
     constexpr int STAGE = pcol16_stage_bytes<N, NBT>();
     constexpr int NST = pcol16_stages<N, NBT>();
+    constexpr int HNB = NB / 2;                      // columns of a half tile
+    constexpr bool HALVES = SPLIT && HNB * 8 >= 16;  // half-tile rows are whole 16-byte TMA units
     uint64_t *bars = reinterpret_cast<uint64_t *>(sbuf);   // NST barriers in the first 128 bytes
     unsigned char *stages = sbuf + 128;
     const int b = threadIdx.x % NB, l = threadIdx.x / NB;
-    const int n_items = L->n;
+    const int n_tiles = L->n;
+    const int n_split = (HALVES && L->items == nullptr) ? L->n_split : 0;
+    const int n_items = n_tiles + n_split;
     __shared__ int s_item[NST];   // item whose tile each stage receives (n_items: none); thread 0 writes
 
     LiveWalker walk(jobs, L);
+    walk.n = n_items;
     auto issue = [&](int item, int s) {   // one thread
         const WorkItem wi = walk.at(item);
         const JobDev &J = jobs[wi.job];
         unsigned char *st = stages + s * STAGE;
-        const int x0 = wi.tile * NB;
-        mbar_arrive_expect_tx(&bars[s], (uint32_t)XB);
-        for (int r0 = 0; r0 < N; r0 += BR) tma_load_2d(st + (size_t)r0 * NB * 8, &J.tmX, x0, r0, &bars[s]);
+        const ColItem ci = col_item(item, n_tiles, n_split);
+        if (!HALVES || ci.half < 0) {
+            const int x0 = wi.tile * NB;   // items == nullptr: the item is the tile
+            mbar_arrive_expect_tx(&bars[s], (uint32_t)XB);
+            for (int r0 = 0; r0 < N; r0 += BR) tma_load_2d(st + (size_t)r0 * NB * 8, &J.tmX, x0, r0, &bars[s]);
+        } else {
+            const int x0 = ci.tile * NB + ci.half * HNB;
+            mbar_arrive_expect_tx(&bars[s], (uint32_t)(XB / 2));
+            for (int r0 = 0; r0 < N; r0 += BR) tma_load_2d(st + (size_t)r0 * HNB * 8, &J.tmXh, x0, r0, &bars[s]);
+        }
     };
 
     int item = walk.next(blockIdx.x);
@@ -2163,72 +2191,131 @@ k_col_p16(const JobDev *jobs, const WorkList *L)
         it_next = it;
     }
     __syncthreads();
+    // thread 0, after the forward transform of item k: request the next item
+    // into the stage of item k - 1, free once the store committed after it
+    // has read it
+    auto request_next = [&](int k) {
+        const int t = (k + NST - 1) % NST;
+        s_item[t] = it_next;
+        if (it_next < n_items) {
+            bulk_wait_read0();
+            fence_proxy_async_smem();
+            issue(it_next, t);
+            it_next = walk.next(it_next + gridDim.x);
+        }
+    };
+    // a wait that gave up: this item and the items already requested beyond it
+    // land before the CTA exits (thread 0)
+    auto drain = [&](int k, const JobDev &J) {
+        atomicExch(&J.st->err, 1);
+        for (int d = 0; d < NST - 1; ++d) {
+            const int t = (k + d) % NST;
+            if (d == 0 || s_item[t] < n_items) mbar_wait(&bars[t], (uint32_t)(((k + d) / NST) & 1), kDrainNs);
+        }
+        bulk_wait0();
+    };
     for (int k = 0; item < n_items; ++k) {
         const int s = k % NST;
         const WorkItem wi = walk.at(item);
         const JobDev &J = jobs[wi.job];
         const int W = J.W;
-        const int x = wi.tile * NB + b;
-        const bool ok = x < W;
         const bool guard = J.mode == kModeShrinkWrap;
-        // the modulus goes straight to registers, its latency hidden by the
-        // tile wait and the forward FFT: from the tiled copy (one 128-byte line
-        // per warp and value) when the job has one
-        float mod[V];
-        if (const float *mt = J.Mt) {
-            mt += (size_t)wi.tile * NB * N + b;
+        const ColItem ci = col_item(item, n_tiles, n_split);
+        float *const sX0 = reinterpret_cast<float *>(stages + s * STAGE);
+        if (!HALVES || ci.half < 0) {
+            const int tile = wi.tile;
+            const int x = tile * NB + b;
+            const bool ok = x < W;
+            // the modulus goes straight to registers, its latency hidden by the
+            // tile wait and the forward FFT: from the tiled copy (one 128-byte
+            // line per warp and value) when the job has one
+            float mod[V];
+            if (const float *mt = J.Mt) {
+                mt += (size_t)tile * NB * N + b;
 #pragma unroll
-            for (int m = 0; m < V; ++m) mod[m] = __ldg(mt + (size_t)(l + m * Q) * NB);
-        } else {
+                for (int m = 0; m < V; ++m) mod[m] = __ldg(mt + (size_t)(l + m * Q) * NB);
+            } else {
 #pragma unroll
-            for (int m = 0; m < V; ++m) mod[m] = ok ? __ldg(J.M + (size_t)(l + m * Q) * W + x) : 0.f;
-        }
-        const bool landed = mbar_wait(&bars[s], (uint32_t)((k / NST) & 1), J.wait_ns);
-        if (__syncthreads_or(!landed)) {
+                for (int m = 0; m < V; ++m) mod[m] = ok ? __ldg(J.M + (size_t)(l + m * Q) * W + x) : 0.f;
+            }
+            const bool landed = mbar_wait(&bars[s], (uint32_t)((k / NST) & 1), J.wait_ns);
+            if (__syncthreads_or(!landed)) {
+                if (threadIdx.x == 0) drain(k, J);
+                return;
+            }
+            float2 *sX = reinterpret_cast<float2 *>(sX0);
+            float2 v[V];
+#pragma unroll
+            for (int m = 0; m < V; ++m) v[m] = sX[(l + m * Q) * NB + b];
+            reg16_fft<N, ColSwz16<N, NB>, -1>(v, sX, b, l, rtw);
+            if (threadIdx.x == 0) request_next(k);
+#pragma unroll
+            for (int m = 0; m < V; ++m) {
+                const float f = modulus_factor(mod[m], v[m], guard);
+                v[m] = make_float2(__fmul_rn(v[m].x, f), __fmul_rn(v[m].y, f));
+            }
+            reg16_fft<N, ColSwz16<N, NB>, +1>(v, sX, b, l, rtw);
+            // the result goes back into the stage (tile layout) and leaves by TMA
+            __syncthreads();
+#pragma unroll
+            for (int m = 0; m < V; ++m) sX[(l + m * Q) * NB + b] = v[m];
+            fence_proxy_async_smem();
+            __syncthreads();
             if (threadIdx.x == 0) {
-                atomicExch(&J.st->err, 1);
-                // this tile and the tiles already requested beyond it land before the CTA exits
-                for (int d = 0; d < NST - 1; ++d) {
-                    const int t = (k + d) % NST;
-                    if (d == 0 || s_item[t] < n_items) mbar_wait(&bars[t], (uint32_t)(((k + d) / NST) & 1), kDrainNs);
-                }
-                bulk_wait0();
+                for (int r0 = 0; r0 < N; r0 += BR) tma_store_2d(&J.tmX, tile * NB, r0, sX + (size_t)r0 * NB);
+                bulk_commit();
             }
-            return;
-        }
-        unsigned char *stg = stages + s * STAGE;
-        float2 *sX = reinterpret_cast<float2 *>(stg);
-        float2 v[V];
+        } else if constexpr (HALVES) {
+            // a half tile: two threads per sequence position, each with the
+            // values of one parity (reg16h_fft), h uniform over a warp; the
+            // stage's second half holds the radix-16 trades (forward, inverse)
+            const int h = (threadIdx.x >> 5) & 1;
+            const int pair = (threadIdx.x & 31) | ((threadIdx.x >> 6) << 5);
+            constexpr int npairs = pcol16_threads(N, NBT) / 2;
+            const int hb = pair % HNB, hl = pair / HNB;
+            const int tile = ci.tile;
+            const int x0 = tile * NB + ci.half * HNB;
+            const int x = x0 + hb;
+            const bool ok = x < W;
+            RegTw16<N> htw;
+            htw.load(J.pcol.tw, hl);
+            float mod[8];
+            if (const float *mt = J.Mt) {
+                mt += (size_t)tile * NB * N + ci.half * HNB + hb;
 #pragma unroll
-        for (int m = 0; m < V; ++m) v[m] = sX[(l + m * Q) * NB + b];
-        reg16_fft<N, ColSwz16<N, NB>, -1>(v, sX, b, l, rtw);
-        if (threadIdx.x == 0) {
-            // the stage of tile k - 1: free once the store committed after it has read it
-            const int t = (k + NST - 1) % NST;
-            s_item[t] = it_next;
-            if (it_next < n_items) {
-                bulk_wait_read0();
-                fence_proxy_async_smem();
-                issue(it_next, t);
-                it_next = walk.next(it_next + gridDim.x);
+                for (int j = 0; j < 8; ++j) mod[j] = __ldg(mt + (size_t)(hl + (2 * j + h) * Q) * NB);
+            } else {
+#pragma unroll
+                for (int j = 0; j < 8; ++j) mod[j] = ok ? __ldg(J.M + (size_t)(hl + (2 * j + h) * Q) * W + x) : 0.f;
             }
-        }
+            const bool landed = mbar_wait(&bars[s], (uint32_t)((k / NST) & 1), J.wait_ns);
+            if (__syncthreads_or(!landed)) {
+                if (threadIdx.x == 0) drain(k, J);
+                return;
+            }
+            float2 *sX = reinterpret_cast<float2 *>(sX0);
+            float2 *mid = sX + N * HNB;   // 2 x 8 * npairs values
+            float2 v[8];
 #pragma unroll
-        for (int m = 0; m < V; ++m) {
-            const float f = modulus_factor(mod[m], v[m], guard);
-            v[m] = make_float2(__fmul_rn(v[m].x, f), __fmul_rn(v[m].y, f));
-        }
-        reg16_fft<N, ColSwz16<N, NB>, +1>(v, sX, b, l, rtw);
-        // the result goes back into the stage (tile layout) and leaves by TMA
-        __syncthreads();
+            for (int j = 0; j < 8; ++j) v[j] = sX[(hl + (2 * j + h) * Q) * HNB + hb];
+            reg16h_fft<N, ColSwz16<N, HNB>, -1>(v, sX, mid, hb, hl, h, pair, npairs, htw);
+            if (threadIdx.x == 0) request_next(k);
 #pragma unroll
-        for (int m = 0; m < V; ++m) sX[(l + m * Q) * NB + b] = v[m];
-        fence_proxy_async_smem();
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            const int x0 = wi.tile * NB;
-            for (int r0 = 0; r0 < N; r0 += BR) tma_store_2d(&J.tmX, x0, r0, sX + (size_t)r0 * NB);
-            bulk_commit();
+            for (int j = 0; j < 8; ++j) {
+                const float f = modulus_factor(mod[j], v[j], guard);
+                v[j] = make_float2(__fmul_rn(v[j].x, f), __fmul_rn(v[j].y, f));
+            }
+            reg16h_fft<N, ColSwz16<N, HNB>, +1>(v, sX, mid + 8 * npairs, hb, hl, h, pair, npairs, htw);
+            __syncthreads();
+#pragma unroll
+            for (int j = 0; j < 8; ++j) sX[(hl + (2 * j + h) * Q) * HNB + hb] = v[j];
+            fence_proxy_async_smem();
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                if (x0 < W)
+                    for (int r0 = 0; r0 < N; r0 += BR) tma_store_2d(&J.tmXh, x0, r0, sX + (size_t)r0 * HNB);
+                bulk_commit();
+            }
         }
         item = s_item[(k + 1) % NST];   // written before the barriers above
     }

@@ -58,6 +58,29 @@ def test_mixed_batch_equals_alone(cuda):
     eng.close()
 
 
+def test_half_tile_column_pass(cuda):
+    """A plan whose column tiles fill at most half of the resident CTAs runs each
+    tile as two half tiles (two threads per 16-value column sequence, one parity
+    each); the engine runs the same jobs as whole tiles.  Both give the same bits,
+    also where a half tile lies partly or wholly past the image's width (260 x 256
+    and 200 x 512: the last tile's second half is outside the image)."""
+    shapes = [(256, 256), (512, 512), (260, 256), (200, 512), (128, 128), (512, 256)]
+    inputs = []
+    for i, (W, H) in enumerate(shapes):
+        M, _ = data.make_modulus(data.BlobSpec(W, H, 12, 0.15 * min(W, H), (1.0, 3.0), (0.3, 1.0), 1e8), 9, i)
+        inputs.append((M, imr.Params(3, FLT_MIN, 0.9, 0.04, 0.2, 3.0, 0.01, 4)))
+    eng = imr.Engine()
+    for i, (M, p) in enumerate(inputs):
+        eng.submit(M, p, tag=i)
+    eng.run()
+    res = {r["tag"]: r for r in eng.poll()}
+    eng.close()
+    for i, (M, p) in enumerate(inputs):
+        alone, n = _alone(M, p)
+        assert res[i]["status"] == 0 and n == p.n_cycles
+        np.testing.assert_array_equal(res[i]["out"], alone, err_msg=str(shapes[i]))
+
+
 def test_several_cycles_per_step(cuda):
     """Four cycles per step graph: the same bits as one request alone, about a
     quarter of the steps, and no step queued after the last request's final
