@@ -37,6 +37,8 @@ def aligned_rel_l2(a: np.ndarray, b: np.ndarray) -> float:
 
 
 def rel_l2(a: np.ndarray, b: np.ndarray) -> float:
-    a = np.asarray(a, np.float64)
-    b = np.asarray(b, np.float64)
+    """||a - b|| / ||b|| in double precision (complex128 when either is complex)."""
+    a, b = np.asarray(a), np.asarray(b)
+    dt = np.complex128 if np.iscomplexobj(a) or np.iscomplexobj(b) else np.float64
+    a, b = a.astype(dt), b.astype(dt)
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))

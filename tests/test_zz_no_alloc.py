@@ -8,10 +8,11 @@ output buffer.
 
 Checked through the C ABI against the existing entry point (the plan API),
 on two calls in a row that reuse the shared array: the second call must not
-see the first one's state.  Both entry points run the same kernels in the
-same order over the same data (the modulus copied, its column tiles built,
-the same launch shapes), so the results must be bit-identical: a tolerance
-would hide an ordering difference.  Runs alone in a fresh process and after
+see the first one's state.  Both entry points do the same arithmetic in the
+same order over the same data (the modulus copied, its column tiles built;
+a plan may run a column tile as two half tiles, which compute the same
+operations), so the results must be bit-identical: a tolerance would hide an
+ordering difference.  Runs alone in a fresh process and after
 the rest of the suite (this file is collected last).
 """
 import ctypes as C
