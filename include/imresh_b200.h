@@ -296,8 +296,11 @@ int imr_shrink_wrap_noalloc_stats(void *stream, int *cycles_done, float *errors,
  * and retires finished ones (their Re(g') is copied to the caller's h_out).
  * Finishing is decided on the device; the host reads every job's state
  * asynchronously and acts on it two steps later, so a step returns without
- * waiting for the GPU (at most two steps are queued).  Not thread safe: drive
- * one engine from one thread.
+ * waiting for the GPU (at most two steps are queued).  Results reach a
+ * pageable h_out through pinned host staging that a helper thread of the
+ * engine pins ahead of need (room for the resident requests' results, at
+ * most 1 GiB, kept until imr_engine_destroy); a pinned h_out is written
+ * directly.  Not thread safe: drive one engine from one thread.
  */
 typedef struct imr_engine imr_engine;
 
