@@ -303,6 +303,7 @@ def _engine_sigs(L):
     vp = C.c_void_p
     L.imr_engine_create.argtypes = [C.POINTER(vp), C.c_size_t, C.c_int, vp]
     L.imr_engine_submit.argtypes = [vp, vp, vp, C.c_uint, C.c_uint, C.POINTER(CParams), C.c_longlong]
+    L.imr_engine_submit_intensity.argtypes = [vp, vp, vp, C.c_uint, C.c_uint, C.POINTER(CParams), C.c_longlong]
     L.imr_engine_step.argtypes = [vp]
     L.imr_engine_run.argtypes = [vp]
     L.imr_engine_poll.argtypes = [vp, C.POINTER(CResult), C.c_int, C.POINTER(C.c_int)]
@@ -339,14 +340,16 @@ class Engine:
         self._keep = {}
 
     def submit(self, modulus: np.ndarray, params: Params | None = None, tag: int = 0,
-               out: np.ndarray | None = None) -> np.ndarray:
+               out: np.ndarray | None = None, intensity: bool = False) -> np.ndarray:
+        """Queue one reconstruction of `modulus` ([H, W]); with intensity=True the
+        array is a measured intensity and the engine takes its square root."""
         m = np.ascontiguousarray(modulus, dtype=np.float32)
         H, W = m.shape
         if out is None:
             out = np.empty_like(m)
         cp = (params or Params()).c()
-        _check(lib().imr_engine_submit(self._h, m.ctypes.data, out.ctypes.data, W, H,
-                                       C.byref(cp), tag), "imr_engine_submit")
+        name = "imr_engine_submit_intensity" if intensity else "imr_engine_submit"
+        _check(getattr(lib(), name)(self._h, m.ctypes.data, out.ctypes.data, W, H, C.byref(cp), tag), name)
         self._keep[tag] = (m, out)
         return out
 

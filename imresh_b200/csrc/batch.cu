@@ -104,6 +104,7 @@ struct EJob {
     int status = IMR_SUCCESS;
     long admit_step = -1;       // its state was set before this step's state copy: older copies are stale
     long cycles_launched = 0;   // cycles queued for it so far (a request ends after n_cycles + 1)
+    bool intensity = false;     // h_in is a measured intensity: the modulus is its square root
     long copy_step = -1;        // retiring: its result copy precedes this step's status copy
     int staging = -1;           // retiring: index of its pinned staging chunk (-1: direct copy)
     size_t staging_off = 0;     // its place in that chunk
@@ -336,6 +337,14 @@ static void reserve_for(imr_engine *E)
     }
 }
 
+// The modulus of a request submitted as a measured intensity: M = sqrt(I),
+// correctly rounded (sqrtf), in place.
+static __global__ void k_sqrt_inplace(float *v, size_t n)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        v[i] = sqrtf(v[i]);
+}
+
 static int admit(imr_engine *E)
 {
     reserve_for(E);
@@ -383,6 +392,14 @@ static int admit(imr_engine *E)
         if (j->resume.empty()) {
             CKE(cudaMemsetAsync(E->dst + j->slot, 0, sizeof(JobState), E->s));
             CKE(cudaMemcpyAsync((void *)j->J.M, j->h_in, (size_t)j->W * j->H * 4, cudaMemcpyHostToDevice, E->s));
+            if (j->intensity) {
+                const size_t n = (size_t)j->W * j->H;
+                k_sqrt_inplace<<<(unsigned)std::min<size_t>((n + 255) / 256, (size_t)E->sms * 8), 256, 0, E->s>>>(
+                    const_cast<float *>(j->J.M), n);
+                CKE(cudaGetLastError());
+                ++E->launches;
+                ++E->host_launches;
+            }
             if ((rc = job_modulus_tiles(j->J, E->s))) return rc;
             if (j->J.Mt) {
                 ++E->launches;
@@ -1073,10 +1090,10 @@ int imr_engine_create(imr_engine **out, size_t device_bytes, int max_jobs, void 
     return IMR_SUCCESS;
 }
 
-int imr_engine_submit(imr_engine *E, const float *h_modulus, float *h_out, unsigned W, unsigned H,
-                      const imr_params *params, long long tag)
+static int submit(imr_engine *E, const float *h_in, bool intensity, float *h_out, unsigned W, unsigned H,
+                  const imr_params *params, long long tag)
 {
-    if (!E || !h_modulus || !h_out || W == 0 || H == 0) return IMR_ERR_INVALID_VALUE;
+    if (!E || !h_in || !h_out || W == 0 || H == 0) return IMR_ERR_INVALID_VALUE;
     EJob *j = new EJob();
     j->W = W;
     j->H = H;
@@ -1086,12 +1103,25 @@ int imr_engine_submit(imr_engine *E, const float *h_modulus, float *h_out, unsig
         delete j;
         return rc;
     }
-    j->h_in = h_modulus;
+    j->h_in = h_in;
+    j->intensity = intensity;
     j->h_out = h_out;
     j->tag = tag;
     j->t_submit = now_ms();
     E->pending.push_back(j);
     return IMR_SUCCESS;
+}
+
+int imr_engine_submit(imr_engine *E, const float *h_modulus, float *h_out, unsigned W, unsigned H,
+                      const imr_params *params, long long tag)
+{
+    return submit(E, h_modulus, false, h_out, W, H, params, tag);
+}
+
+int imr_engine_submit_intensity(imr_engine *E, const float *h_intensity, float *h_out, unsigned W, unsigned H,
+                                const imr_params *params, long long tag)
+{
+    return submit(E, h_intensity, true, h_out, W, H, params, tag);
 }
 
 int imr_engine_step(imr_engine *E)

@@ -348,6 +348,12 @@ int imr_engine_create(imr_engine **engine, size_t device_bytes, int max_jobs, vo
  * request is admitted, h_out (W*H floats) until its result is polled. */
 int imr_engine_submit(imr_engine *engine, const float *h_modulus, float *h_out, unsigned W,
                       unsigned H, const imr_params *params, long long tag);
+/* The same for a measured intensity I (W*H floats, >= 0): the engine takes
+ * the modulus sqrt(I) (correctly rounded, in FP32) on the device at
+ * admission, so the result equals submitting sqrtf(I).  No counterpart in
+ * the reference (its callers pass the modulus). */
+int imr_engine_submit_intensity(imr_engine *engine, const float *h_intensity, float *h_out, unsigned W,
+                                unsigned H, const imr_params *params, long long tag);
 /* Retire what had finished two steps ago, admit, launch one step (one cycle,
  * or imr_engine_set_cycles_per_step's count) of every active reconstruction.
  * Returns once the step is queued (it waits only for the step before the

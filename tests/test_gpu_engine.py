@@ -81,6 +81,29 @@ def test_half_tile_column_pass(cuda):
         np.testing.assert_array_equal(res[i]["out"], alone, err_msg=str(shapes[i]))
 
 
+def test_submit_intensity_equals_modulus(cuda):
+    """A request submitted as a measured intensity I gives the bits of the same
+    request submitted as the modulus sqrtf(I) (the engine takes the square root
+    at admission), alone and beside modulus requests."""
+    inputs = _inputs()[:6]
+    eng = imr.Engine()
+    for i, (M, p) in enumerate(inputs):
+        eng.submit(M, p, tag=i)
+        I = (M.astype(np.float64) ** 2).astype(np.float32)
+        eng.submit(I, p, tag=100 + i, intensity=True)
+    eng.run()
+    res = {r["tag"]: r for r in eng.poll()}
+    eng.close()
+    for i, (M, p) in enumerate(inputs):
+        I = (M.astype(np.float64) ** 2).astype(np.float32)
+        want = np.sqrt(I)   # float32, correctly rounded
+        alone, _ = _alone(want, p)
+        assert res[100 + i]["status"] == 0
+        np.testing.assert_array_equal(res[100 + i]["out"], alone)
+        if np.array_equal(want, M):
+            np.testing.assert_array_equal(res[100 + i]["out"], res[i]["out"])
+
+
 def test_several_cycles_per_step(cuda):
     """Four cycles per step graph: the same bits as one request alone, about a
     quarter of the steps, and no step queued after the last request's final
