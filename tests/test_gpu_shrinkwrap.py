@@ -45,7 +45,10 @@ def _run_gpu(M, p: oracle.SwParams, cuda_defaults=False):
                                    (97, 130), (211, 64),
                                    # column-tiled modulus: 2-column tiles at length 4096, and a
                                    # last tile of 4 of 16 columns
-                                   (4096, 64), (256, 132)])
+                                   (4096, 64), (256, 132),
+                                   # half-tile column passes whose last tile's second half lies
+                                   # past the width; a Bluestein width over 8-value half tiles
+                                   (512, 520), (128, 1000)])
 def test_one_cycle_matches_oracle(cuda, shape):
     H, W = shape
     M, _ = data.make_modulus(_spec(W, H), 1)
