@@ -775,9 +775,9 @@ def main():
     ap.add_argument("--schedule", type=int, default=0, help="--serve: 0 grouped, 1 chained step graphs")
     ap.add_argument("--step-target", type=float, default=0.0,
                     help="--serve: admission bound from the measured step time, ms (0: off)")
-    ap.add_argument("--ncu-case", type=int, default=0, metavar="N",
-                    help="run one NxN reconstruction (1 cycle x 3 HIO) of the headline recipe scaled to N "
-                         "and exit: a small case for ncu")
+    ap.add_argument("--ncu-case", type=str, default="", metavar="N or WxH",
+                    help="run one NxN (or WxH) reconstruction (1 cycle x 3 HIO) of the headline recipe scaled "
+                         "to that size and exit: a small case for ncu")
     ap.add_argument("--ncu-prec", type=int, default=0,
                     help="column-pass precision of the ncu case (0 FP32, 1 BF16 hi+lo, 2 FP16 hi+lo)")
     args = ap.parse_args()
@@ -785,17 +785,19 @@ def main():
         import torch
         import imresh_b200 as imr
         from imresh_b200 import data
-        n = args.ncu_case
-        # the headline's blob density, radius and Poisson noise, scaled to N x N
-        M, _ = data.make_modulus(data.BlobSpec(n, n, max(1, 400 * n * n // 2048 ** 2), 300.0 * n / 2048,
+        w, _, h = args.ncu_case.partition("x")
+        w = int(w)
+        h = int(h) if h else w
+        # the headline's blob density, radius and Poisson noise, scaled to W x H
+        M, _ = data.make_modulus(data.BlobSpec(w, h, max(1, 400 * w * h // 2048 ** 2), 300.0 * min(w, h) / 2048,
                                                (1.5, 3.0), (0.3, 1.0), 1e9), 0)
-        plan = imr.Plan(n, n, imr.Params(1, imr.FLT_MIN, 0.9, 0.04, 0.2, 3.0, 0.01, 3))
+        plan = imr.Plan(w, h, imr.Params(1, imr.FLT_MIN, 0.9, 0.04, 0.2, 3.0, 0.01, 3))
         plan.set_precision(args.ncu_prec)
         d_m = torch.from_numpy(M).cuda()
         d_o = torch.empty_like(d_m)
         plan.execute(d_m, d_o)
         torch.cuda.synchronize()
-        print(json.dumps({"ncu_case": n, "precision": args.ncu_prec, "checksum": float(d_o.abs().sum())}))
+        print(json.dumps({"ncu_case": [w, h], "precision": args.ncu_prec, "checksum": float(d_o.abs().sum())}))
         return
     if args.serve:
         import torch
