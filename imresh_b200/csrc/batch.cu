@@ -812,7 +812,15 @@ static void stage_request(imr_engine *E)
         if (g.have >= g.want) return;
         g.credit = 1;
     }
-    if (!g.th.joinable()) g.th = std::thread(grower_main, E);
+    if (!g.th.joinable()) {
+        try {
+            g.th = std::thread(grower_main, E);
+        } catch (...) {   // no thread: staging is allocated on demand, as without the helper
+            std::lock_guard<std::mutex> lk(g.mu);
+            g.failed = true;
+            return;
+        }
+    }
     g.cv.notify_one();
 }
 
@@ -896,11 +904,22 @@ static void hand_over(std::vector<HandOver> &h)
         for (const HandOver &x : h) memcpy(x.dst, x.src, x.bytes);
         return;
     }
+    // thread t copies results t, t + nt, ...; results of threads that could not
+    // be started are copied here
     std::vector<std::thread> th;
-    for (size_t t = 0; t < nt; ++t)
-        th.emplace_back([&h, t, nt] {
-            for (size_t i = t; i < h.size(); i += nt) memcpy(h[i].dst, h[i].src, h[i].bytes);
-        });
+    size_t started = 0;
+    for (size_t t = 0; t < nt; ++t) {
+        try {
+            th.emplace_back([&h, t, nt] {
+                for (size_t i = t; i < h.size(); i += nt) memcpy(h[i].dst, h[i].src, h[i].bytes);
+            });
+            ++started;
+        } catch (...) {
+            break;
+        }
+    }
+    for (size_t t = started; t < nt; ++t)
+        for (size_t i = t; i < h.size(); i += nt) memcpy(h[i].dst, h[i].src, h[i].bytes);
     for (auto &x : th) x.join();
 }
 
