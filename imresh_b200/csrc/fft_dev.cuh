@@ -292,6 +292,30 @@ __device__ __forceinline__ void dft7(float2 *v)
     for (int k = 0; k < 7; ++k) v[k] = y[k];
 }
 
+// 12 points by the prime-factor (Good-Thomas) split 3 x 4, which needs no
+// twiddles: input index n = (4 n1 + 3 n2) mod 12, DFT-3 over n1, DFT-4 over n2,
+// output index k = (4 k1 + 9 k2) mod 12 (k1 = k mod 3, k2 = k mod 4), since
+// n k = 4 n1 k1 + 3 n2 k2 (mod 12).
+template <int S>
+__device__ __forceinline__ void dft12(float2 *v)
+{
+    float2 A[4][3];
+#pragma unroll
+    for (int n2 = 0; n2 < 4; ++n2) {
+        float2 a[3] = {v[(3 * n2) % 12], v[(4 + 3 * n2) % 12], v[(8 + 3 * n2) % 12]};
+        dft3<S>(a);
+#pragma unroll
+        for (int k1 = 0; k1 < 3; ++k1) A[n2][k1] = a[k1];
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < 3; ++k1) {
+        float2 b[4] = {A[0][k1], A[1][k1], A[2][k1], A[3][k1]};
+        dft4<S>(b);
+#pragma unroll
+        for (int k2 = 0; k2 < 4; ++k2) v[(4 * k1 + 9 * k2) % 12] = b[k2];
+    }
+}
+
 template <int R, int S>
 __device__ __forceinline__ void dftR(float2 *v)
 {
@@ -301,6 +325,7 @@ __device__ __forceinline__ void dftR(float2 *v)
     else if constexpr (R == 5) dft5<S>(v);
     else if constexpr (R == 7) dft7<S>(v);
     else if constexpr (R == 16) dft16<S>(v);
+    else if constexpr (R == 12) dft12<S>(v);
     else dft8<S>(v);
 }
 

@@ -21,18 +21,22 @@ namespace imr {
 __host__ __device__ constexpr bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
 
 // Lengths the pipelined register FFT handles: powers of two (8 values per
-// thread, radices 8/4/2) and 3 * 2^k (12 values per thread, radices 4/2/3).
+// thread, radices 8/4/2) and 3 * 2^k (12 values per thread, radices 12/4/2).
 __host__ __device__ constexpr bool is_3pow2(int n) { return n >= 48 && n % 3 == 0 && is_pow2(n / 3); }
 __host__ __device__ constexpr int reg_v(int n) { return is_pow2(n) ? 8 : 12; }
 __host__ __device__ constexpr RadixList reg_radix_list(int n)
 {
     if (is_pow2(n)) return radix_list(n);
     RadixList L{0, {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0}};
-    int k = 0, m = n / 3;
+    int k = 0, m = n % 12 == 0 ? n / 12 : n / 3;
     while (m > 1) { m >>= 1; ++k; }
+    // 3*2^k >= 12: a first, twiddle-free radix-12 pass (prime-factor 3 x 4),
+    // then radix 4 and at most one radix 2 -- one pass, and one shared-memory
+    // exchange, fewer than radix 4 ... 4, 3
+    if (n % 12 == 0) L.r[L.n++] = 12;
     for (; k >= 2; k -= 2) L.r[L.n++] = 4;
     if (k == 1) L.r[L.n++] = 2;
-    L.r[L.n++] = 3;
+    if (n % 12 != 0) L.r[L.n++] = 3;
     return L;
 }
 

@@ -1663,10 +1663,12 @@ template <bool FIRST, int N>
 __host__ __device__ constexpr int prow_smem() { return 128 + 2 * prow_stage_bytes<FIRST, N>(); }
 // Three 8-warp CTAs per SM for the every-iteration shrink-wrap pass at
 // power-of-two lengths (its stages fit three times in shared memory; 80
-// registers per thread, no spills).  Other variants keep their registers.
+// registers per thread, no spills), two at lengths 3 * 2^k (stages of up to
+// 52 KB; left free, the compiler took up to 246 registers, one CTA per SM).
+// Other variants keep their registers.
 __host__ __device__ constexpr int prow_min_blocks(bool FIRST, bool FIX, int N)
 {
-    return !FIRST && !FIX && is_pow2(N) && N <= 2048 ? 3 : 1;
+    return !FIRST && !FIX && is_pow2(N) && N <= 2048 ? 3 : (!FIRST && !FIX && N % 3 == 0 ? 2 : 1);
 }
 
 __device__ __forceinline__ bool job_live(const JobDev *jobs, const WorkList *L, int item)
